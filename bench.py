@@ -1,0 +1,322 @@
+"""Benchmark of the fused HiPIMS step on the synthetic urban catchment.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the configuration the headline metric is quoted on): a 2048 x 2048
+urban catchment, 2 m cells, seeded Gaussian-random-field DEM (k^-3, 0-50 m)
+with 8 % of cells raised 10 m as buildings, 30 % road cells (n = 0.035, else
+0.08), open boundary ring, dry start, uniform rain 50 mm/h.  A step is one
+fused launch advancing every valid cell (4,194,304) by one time step.
+
+Timing: 8 untimed spin-up steps (the dry start becomes wet everywhere), W
+untimed warm-up steps, then K timed steps.  Each timed step is bracketed by
+CUDA events on the launching stream; a 256 MiB buffer is written between timed
+steps to flush the 126 MB L2.  N > 1 (torchrun): every rank advances its own
+replica (weak scaling; the catchment does not shard without a halo exchange),
+the time is the max over ranks and `value` counts the cells of all ranks.
+
+--impl reference times the reference's own HiPIMS kernels compiled for the
+host (oracle/_ref) under the reference's step order on this machine's CPU
+cores, on the same catchment.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "chans-hipims-flamegpu_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+METRIC = "Gcell-updates/s"
+N_CELLS = 2048
+SPINUP = 8
+BYTES_PER_CELL_FP32 = 37  # read h,qx,qy,z,h_max (5 x 4) + code (1); write h,qx,qy,h_max (4 x 4)
+FALLBACK_HBM_GBS = 6650.0
+
+
+def workload(n: int = N_CELLS) -> dict:
+    from hipims_b200 import scenarios as S
+
+    return S.urban_catchment(n, dx=2.0, seed=0)
+
+
+def config_of(n: int, world: int, extra: dict | None = None) -> dict:
+    cfg = {"workload": f"urban catchment {n}x{n}, 2 m cells, GRF DEM + 8% buildings, "
+                       f"2 Manning zones, open ring, dry start, rain 50 mm/h",
+           "cells_per_instance": n * n, "instances_per_gpu": 1,
+           "parallelism": f"replicas x{world}", "spinup_steps": SPINUP,
+           "l2": "flushed between timed steps (256 MiB write)"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+
+    def __init__(self, gpu: int):
+        self.path = tempfile.mktemp(suffix=".csv")
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(gpu), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for ln in f:
+                parts = [p.strip() for p in ln.split(",")]
+                if len(parts) >= 7:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[3 + k] == "Active"})
+        busy = [s for s in sm if mx and s > 0.5 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(busy) if busy else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def measured_peak() -> tuple[float, str]:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic() -> float | None:
+    """DRAM bytes per fused-step launch from the committed ncu summary, if any."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "fused_step_traffic.json")) as f:
+            return float(json.load(f)["dram_bytes_per_launch_full_size"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def cpu_reference_rate(d: dict, steps: int, warmup: int, threads: int | None = None) -> dict:
+    """Cells x steps / s of the reference's host-built kernels (or the
+    restatement when oracle/_ref is absent) on catchment d."""
+    from oracle import oracle as O
+
+    kind = "reference" if O.ref_available() else "port"
+    threads = threads or os.cpu_count() or 1
+    O.set_threads(threads)
+    sim = O.Sim(d, order=2, backend="ref" if kind == "reference" else "oracle")
+    sim.run(SPINUP + warmup)
+    t0 = time.perf_counter()
+    sim.run(steps)
+    el = time.perf_counter() - t0
+    return {"value": sim.N * steps / el / 1e9, "unit": METRIC, "cores": threads, "kind": kind,
+            "seconds": el, "steps": steps,
+            "sample": f"{steps} steps of the full {int(np.sqrt(sim.N))}^2 catchment after "
+                      f"{SPINUP + warmup} untimed steps, FP64, {threads} threads"}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    d = workload(args.cells)
+    cb = cpu_reference_rate(d, args.steps, args.warmup)
+    line = {"metric": METRIC, "value": cb["value"], "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": cb["seconds"] / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference", "config": config_of(args.cells, 1),
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": METRIC, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import torch.distributed as dist
+
+    from hipims_b200 import _lib
+    from hipims_b200.fused import FusedSolver
+    from hipims_b200.scenarios import catchment_from
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    d = workload(args.cells)
+    fs = FusedSolver(catchment_from(d), dtype=torch.float32, tile=tuple(args.tile), device=dev)
+    n_valid = fs.inst[0].n_valid
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    fs.step(SPINUP + args.warmup)
+    torch.cuda.synchronize(dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    clocks = Clocks(local)
+    barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    for a, b in ev:
+        flush.fill_(1)
+        a.record(stream)
+        fs.step(1)
+        b.record(stream)
+    barrier()
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * n_valid * args.steps / (total_ms * 1e-3) / 1e9
+    c = fs.controls()[0]
+
+    # end to end through the C ABI with host buffers: H2D of the state from
+    # pinned memory, one fused step, D2H of the new state, every step
+    ins = fs.inst[0]
+    host_in = [torch.empty_like(x, device="cpu").pin_memory() for x in (ins.h[0], ins.qx[0],
+                                                                        ins.qy[0])]
+    host_out = [torch.empty_like(x) for x in host_in]
+    for hsrc, x in zip(host_in, (ins.h[c.cur], ins.qx[c.cur], ins.qy[c.cur])):
+        hsrc.copy_(x)
+    cur = c.cur
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        for hsrc, x in zip(host_in, (ins.h[cur], ins.qx[cur], ins.qy[cur])):
+            x.copy_(hsrc, non_blocking=True)
+        fs.step(1)
+        cur = 1 - cur
+        for hdst, x in zip(host_out, (ins.h[cur], ins.qx[cur], ins.qy[cur])):
+            hdst.copy_(x, non_blocking=True)
+    e1.record(stream)
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = world * n_valid * args.steps / (e2e_ms * 1e-3) / 1e9
+    bytes_io = sum(x.numel() * x.element_size() for x in host_in)
+
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        avg_s = total_ms / args.steps * 1e-3
+        alg_bytes = BYTES_PER_CELL_FP32 * n_valid
+        achieved = alg_bytes / avg_s / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "ours",
+            "config": config_of(args.cells, world, {"tile": list(args.tile),
+                                                     "sim_time_s": c.t, "dt_s": c.dt}),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "kernel": "fused_step_kernel<float,32,32>",
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "traffic": profiled_traffic()},
+            "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": bytes_io,
+                    "d2h_bytes_per_step": bytes_io},
+            "gpu_launches": args.steps,
+            "clocks": clk,
+            "step_ms_min": min(step_ms), "step_ms_max": max(step_ms),
+        }
+        if args.accuracy:
+            line["accuracy"] = accuracy_vs_fp64(d, dev, SPINUP + args.warmup + args.steps)
+        if args.cpu_baseline and world == 1:
+            line["cpu_baseline"] = {k: v for k, v in cpu_reference_rate(
+                d, args.cpu_steps, 0).items() if k in ("value", "unit", "cores", "kind",
+                                                       "sample")}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    del _lib
+
+
+def accuracy_vs_fp64(d: dict, dev, steps: int) -> dict:
+    """Max depth / velocity difference of the FP32 fused run against the FP64
+    fused run at identical simulated times (the FP64 dt sequence replayed), and
+    the FP64 volume balance of the FP32 run."""
+    from hipims_b200.fused import FusedSolver
+    from hipims_b200.scenarios import catchment_from
+
+    f64 = FusedSolver(catchment_from(d), dtype=torch.float64, device=dev)
+    dts = []
+    for _ in range(steps):
+        f64.step(1)
+        dts.append(f64.controls()[0].dt)
+    f32 = FusedSolver(catchment_from(d, dt_replay=np.asarray(dts)), dtype=torch.float32,
+                      device=dev)
+    f32.step(steps)
+    a, b = f32.compacted(), f64.compacted()
+    wet = b["h"] > 1e-3
+    ua = np.where(wet, a["qx"] / np.maximum(a["h"], 1e-3), 0)
+    ub = np.where(wet, b["qx"] / np.maximum(b["h"], 1e-3), 0)
+    c = f32.controls()[0]
+    bal = abs(c.volume - c.volume0 - c.rain_volume + c.outflow_volume) / max(c.rain_volume,
+                                                                               1e-30)
+    return {"steps": steps, "sim_time_s": c.t, "max_abs_dh_m": float(np.abs(a["h"] - b["h"]).max()),
+            "max_abs_du_ms_wet": float(np.abs(ua - ub).max()),
+            "volume_balance_rel_err": bal, "reference": "FP64 fused run, same dt sequence"}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cells", type=int, default=N_CELLS)
+    ap.add_argument("--tile", type=int, nargs=2, default=[32, 32])
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-accuracy", dest="accuracy", action="store_false")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,350 @@
+"""FusedSolver: dense-tile, one-kernel-per-step HiPIMS solver (single or batched).
+
+A catchment is given as rasters (type-code mask, z, h, qx, qy, Manning zone)
+exactly as the reference's ``Godunov.init__fluidField_tensor`` takes them; the
+solver keeps them dense (no compaction, no neighbour table) in the padded
+layout of include/hipims_b200_fused.h and advances every instance of a batch
+with one ``hb_fused_step`` launch per step.  ``t`` and ``dt`` live in a device
+control block per instance, so K steps can be enqueued (or replayed from a
+CUDA graph) without a host sync.
+
+Semantics follow the reference step (HP/SWE_CUDA.py:339-424, 497-502,
+780-831): the same activity mask, MUSCL/hydrostatic/HLLC fluxes, bed slope,
+rain, implicit friction, CFL step with the 10x growth cap and the clip to
+export times.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import math
+from typing import Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from .topology import decode_bc
+
+
+@dataclasses.dataclass
+class Catchment:
+    """One instance.  Rasters are [rows, cols]; mask > 0 marks valid cells and
+    holds the reference type code (1 interior, e.g. 50 = OPEN id 0)."""
+
+    mask: np.ndarray
+    z: np.ndarray
+    h: np.ndarray
+    qx: np.ndarray | None = None
+    qy: np.ndarray | None = None
+    zone: np.ndarray | None = None          # Manning zone per cell (< 16)
+    manning: Sequence[float] = (0.03,)
+    dx: float = 1.0
+    cfl: float = 0.5
+    t0: float = 0.0
+    dt0: float = 1.0e-4
+    export_step: float = 0.0                # 0: no export clipping
+    t_end: float = math.inf
+    halt_on_export: bool = False
+    rain: np.ndarray | None = None          # [T, 2] time (s), rate (m/s)
+    rain_mult: float = 1.0
+    given_depth: np.ndarray | None = None   # [Td, 1 + nH]
+    given_wl: np.ndarray | None = None      # [Tw, 1 + nW]
+    given_q: np.ndarray | None = None       # [Tq, 1 + 2 nQ]
+    h_max: np.ndarray | None = None         # default: h
+    dt_replay: np.ndarray | None = None     # frozen schedule: dt of step k+1 = dt_replay[k]
+
+
+def _round_up(x: int, m: int) -> int:
+    return (x + m - 1) // m * m
+
+
+class _Instance:
+    """Device arrays of one catchment in the padded dense layout."""
+
+    def __init__(self, c: Catchment, dtype: torch.dtype, device, tile: tuple[int, int]):
+        rows, cols = c.mask.shape
+        self.rows, self.cols = rows, cols
+        self.dx = float(c.dx)
+        ty, tx = tile
+        self.tiles_y = (rows + ty - 1) // ty
+        self.tiles_x = (cols + tx - 1) // tx
+        rows_s = _round_up(rows, 64) + 2 * _lib.HB_PAD_Y
+        pitch = _round_up(_round_up(cols, 64) + 2 * _lib.HB_PAD_X, 32)
+        code_pitch = _round_up(_round_up(cols, 64) + 2 * _lib.HB_CODE_PAD_X, 128)
+        self.rows_s, self.pitch, self.code_pitch = rows_s, pitch, code_pitch
+        PY, PX, CPX = _lib.HB_PAD_Y, _lib.HB_PAD_X, _lib.HB_CODE_PAD_X
+        mask = np.asarray(c.mask)
+        valid = mask > 0
+        self.valid = valid
+        self.n_valid = int(valid.sum())
+
+        # boundary classes: distinct type codes of valid cells
+        codes = sorted(set(int(v) for v in np.unique(mask[valid])))
+        if len(codes) > _lib.HB_MAX_CLASSES - 1:
+            raise ValueError(f"at most {_lib.HB_MAX_CLASSES - 1} distinct cell codes per "
+                             f"catchment in the fused path (got {len(codes)})")
+        self.class_codes = codes
+        cls_of = {code: k for k, code in enumerate(codes)}
+        cls = np.full(mask.shape, _lib.HB_NODATA_CLASS, dtype=np.uint8)
+        for code, k in cls_of.items():
+            cls[mask == code] = k
+        zone = np.zeros(mask.shape, dtype=np.uint8) if c.zone is None else np.asarray(c.zone)
+        if zone.max(initial=0) >= _lib.HB_MAX_ZONES or len(c.manning) > _lib.HB_MAX_ZONES:
+            raise ValueError(f"at most {_lib.HB_MAX_ZONES} Manning zones in the fused path")
+        code_r = ((cls.astype(np.uint8) << 4) | (zone.astype(np.uint8) & 15)).astype(np.uint8)
+        code_np = np.full((rows_s, code_pitch), _lib.HB_NODATA_CLASS << 4, dtype=np.uint8)
+        code_np[PY:PY + rows, CPX:CPX + cols] = code_r
+
+        # datum per 64 x 64 block (FP32 only)
+        z = np.asarray(c.z, dtype=np.float64)
+        fp32 = dtype == torch.float32
+        nby, nbx = (rows + 63) // 64, (cols + 63) // 64
+        datum = np.zeros((nby, nbx), dtype=np.float64)
+        if fp32:
+            zv = np.where(valid, z, np.inf)
+            for by in range(nby):
+                for bx in range(nbx):
+                    blk = zv[by * 64:(by + 1) * 64, bx * 64:(bx + 1) * 64]
+                    m = blk.min()
+                    datum[by, bx] = math.floor(m) if np.isfinite(m) else 0.0
+        self.datum_np = datum
+        dfull = np.repeat(np.repeat(datum, 64, axis=0), 64, axis=1)[:rows, :cols]
+        zrel = np.where(valid, z - dfull, 0.0)
+
+        def dense(a, fill=0.0):
+            out = np.full((rows_s, pitch), fill, dtype=np.float64)
+            if a is not None:
+                out[PY:PY + rows, PX:PX + cols] = np.where(valid, np.asarray(a, np.float64), 0.0)
+            return torch.as_tensor(out, dtype=dtype, device=device).contiguous()
+
+        h = dense(c.h)
+        qx = dense(c.qx)
+        qy = dense(c.qy)
+        self.h = [h, h.clone()]
+        self.qx = [qx, qx.clone()]
+        self.qy = [qy, qy.clone()]
+        self.z = dense(zrel)
+        self.h_max = dense(c.h if c.h_max is None else c.h_max)
+        self.code = torch.as_tensor(code_np, device=device).contiguous()
+        self.datum = torch.as_tensor(datum, dtype=torch.float32, device=device).contiguous()
+        self.z_abs_offset = dfull
+
+        def table(a, width):
+            if a is None:
+                a = np.zeros((1, width))
+            a = np.atleast_2d(np.asarray(a, dtype=np.float64))
+            return torch.as_tensor(a, device=device).contiguous()
+
+        self.given_depth = table(c.given_depth, 2)
+        self.given_wl = table(c.given_wl, 2)
+        self.given_q = table(c.given_q, 3)
+        self.rain = None if c.rain is None else table(c.rain, 2)
+        self.dt_replay = None if c.dt_replay is None else torch.as_tensor(
+            np.asarray(c.dt_replay, dtype=np.float64), device=device).contiguous()
+
+        # position of compacted cell 0 (fluxMask quirk)
+        if self.n_valid:
+            flat = int(np.flatnonzero(valid.ravel())[0])
+            self.bug = (flat // cols, flat % cols)
+        else:
+            self.bug = (-1, -1)
+        self.bc_type = [1] * _lib.HB_MAX_CLASSES
+        self.bc_id = [0] * _lib.HB_MAX_CLASSES
+        for code, k in cls_of.items():
+            bt, bid = decode_bc(code)
+            self.bc_type[k] = bt
+            self.bc_id[k] = bid
+        self.manning = list(c.manning) + [0.0] * (_lib.HB_MAX_ZONES - len(c.manning))
+        self.catchment = c
+
+    def raster(self, t: torch.Tensor) -> torch.Tensor:
+        PY, PX = _lib.HB_PAD_Y, _lib.HB_PAD_X
+        return t[PY:PY + self.rows, PX:PX + self.cols]
+
+
+class FusedSolver:
+    """Advance one or more catchments with the fused dense-tile kernel."""
+
+    def __init__(self, catchments: Catchment | Sequence[Catchment], dtype=torch.float32,
+                 tile: tuple[int, int] = (32, 32), device="cuda", grid_blocks: int = 0):
+        if isinstance(catchments, Catchment):
+            catchments = [catchments]
+        if dtype not in (torch.float32, torch.float64):
+            raise ValueError("dtype must be float32 or float64")
+        self.device = torch.device(device)
+        self.dtype = dtype
+        self.tile = tuple(tile)
+        self.inst = [_Instance(c, dtype, self.device, self.tile) for c in catchments]
+        n = len(self.inst)
+        self._ctrl_size = ctypes.sizeof(_lib.HbCtrl)
+        ctrl_host = (_lib.HbCtrl * n)()
+        tile_inst = []
+        begin = 0
+        recs = (_lib.HbInstance * n)()
+        self.ctrl = torch.zeros(n * self._ctrl_size, dtype=torch.uint8, device=self.device)
+        for k, (ins, c) in enumerate(zip(self.inst, catchments)):
+            cb = ctrl_host[k]
+            cb.t, cb.dt = c.t0, c.dt0
+            cb.export_step = c.export_step
+            cb.t_end = c.t_end
+            cb.rain_mult = c.rain_mult
+            cb.halt_on_export = int(c.halt_on_export)
+            r = recs[k]
+            r.rows, r.cols = ins.rows, ins.cols
+            r.tiles_x, r.tiles_y = ins.tiles_x, ins.tiles_y
+            r.tile_begin = begin
+            r.pitch, r.code_pitch = ins.pitch, ins.code_pitch
+            r.datum_ny, r.datum_nx = ins.datum_np.shape
+            r.bug_y, r.bug_x = ins.bug
+            r.h[0], r.h[1] = ins.h[0].data_ptr(), ins.h[1].data_ptr()
+            r.qx[0], r.qx[1] = ins.qx[0].data_ptr(), ins.qx[1].data_ptr()
+            r.qy[0], r.qy[1] = ins.qy[0].data_ptr(), ins.qy[1].data_ptr()
+            r.z = ins.z.data_ptr()
+            r.h_max = ins.h_max.data_ptr()
+            r.code = ins.code.data_ptr()
+            r.datum = ins.datum.data_ptr() if dtype == torch.float32 else None
+            r.ctrl = self.ctrl.data_ptr() + k * self._ctrl_size
+            if ins.rain is not None:
+                r.rain_tab = ins.rain.data_ptr()
+                r.rain_rows, r.rain_cols = ins.rain.shape
+            r.given_depth = ins.given_depth.data_ptr()
+            r.depth_rows, r.depth_cols = ins.given_depth.shape
+            r.given_wl = ins.given_wl.data_ptr()
+            r.wl_rows, r.wl_cols = ins.given_wl.shape
+            r.given_q = ins.given_q.data_ptr()
+            r.q_rows, r.q_cols = ins.given_q.shape
+            r.dx, r.cfl = c.dx, c.cfl
+            for z_ in range(_lib.HB_MAX_ZONES):
+                r.manning[z_] = ins.manning[z_]
+            for q in range(_lib.HB_MAX_CLASSES):
+                r.bc_type[q] = ins.bc_type[q]
+                r.bc_id[q] = ins.bc_id[q]
+            r.n_valid = ins.n_valid
+            if ins.dt_replay is not None:
+                r.dt_replay = ins.dt_replay.data_ptr()
+                r.n_replay = ins.dt_replay.numel()
+            nt = ins.tiles_x * ins.tiles_y
+            tile_inst.extend([k] * nt)
+            begin += nt
+        self.n_tiles = begin
+        self.ctrl.copy_(torch.frombuffer(bytearray(ctrl_host), dtype=torch.uint8))
+        self._recs_host = recs
+        self.records = torch.frombuffer(bytearray(recs), dtype=torch.uint8).to(self.device)
+        self.tile_instance = torch.tensor(tile_inst, dtype=torch.int32, device=self.device)
+        b = _lib.HbFusedBatch()
+        b.dtype = _lib.HB_F32 if dtype == torch.float32 else _lib.HB_F64
+        b.n_instances = n
+        b.n_tiles = self.n_tiles
+        b.tile_y, b.tile_x = self.tile
+        b.grid_blocks = grid_blocks
+        b.order = 2
+        b.instances = self.records.data_ptr()
+        b.tile_instance = self.tile_instance.data_ptr()
+        L = _lib.lib()
+        ws = L.hb_fused_workspace_size(ctypes.byref(b))
+        self.workspace = torch.zeros(max(ws, 256), dtype=torch.uint8, device=self.device)
+        b.workspace = self.workspace.data_ptr()
+        self.batch = b
+        self._graph = None
+        self._graph_steps = 0
+        self.prepare()
+
+    # ----------------------------------------------------------------- control
+    def _stream(self) -> int:
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    def prepare(self) -> None:
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.lib().hb_fused_prepare(ctypes.byref(self.batch), self._stream()),
+                       "hb_fused_prepare")
+
+    def step(self, nsteps: int = 1) -> None:
+        """Enqueue nsteps fused steps (no host sync)."""
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.lib().hb_fused_step(ctypes.byref(self.batch), int(nsteps),
+                                                self._stream()), "hb_fused_step")
+
+    def capture(self, nsteps: int) -> None:
+        """Capture nsteps steps in a CUDA graph for replay()."""
+        self._graph = None
+        torch.cuda.synchronize(self.device)
+        s = torch.cuda.Stream(self.device)
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                _lib.check(_lib.lib().hb_fused_step(ctypes.byref(self.batch), int(nsteps),
+                                                    s.cuda_stream), "hb_fused_step")
+        torch.cuda.current_stream(self.device).wait_stream(s)
+        self._graph = g
+        self._graph_steps = nsteps
+
+    def replay(self) -> None:
+        if self._graph is None:
+            raise RuntimeError("capture() first")
+        self._graph.replay()
+
+    def controls(self) -> list[_lib.HbCtrl]:
+        """Host copy of every instance's control block (syncs)."""
+        raw = bytearray(self.ctrl.cpu().numpy().tobytes())
+        n = len(self.inst)
+        arr = (_lib.HbCtrl * n).from_buffer_copy(raw)
+        return list(arr)
+
+    def write_controls(self, ctrls: Sequence[_lib.HbCtrl]) -> None:
+        n = len(self.inst)
+        arr = (_lib.HbCtrl * n)(*ctrls)
+        self.ctrl.copy_(torch.frombuffer(bytearray(arr), dtype=torch.uint8))
+
+    def resume(self, k: int | None = None) -> None:
+        """Clear the halted flag (after an export halt) of one or all instances."""
+        cs = self.controls()
+        for i, c in enumerate(cs):
+            if k is None or k == i:
+                c.halted = 0
+        self.write_controls(cs)
+
+    def run_until(self, t_end: float, chunk: int = 64, max_steps: int = 10 ** 9) -> int:
+        """Advance every instance until t >= t_end; returns steps taken (max over instances)."""
+        cs = self.controls()
+        for c in cs:
+            c.t_end = t_end
+            c.halted = 0 if c.t < t_end else 1
+        self.write_controls(cs)
+        start = max(c.step for c in cs)
+        while True:
+            self.step(chunk)
+            cs = self.controls()
+            steps = max(c.step for c in cs) - start
+            if all(c.halted for c in cs) or steps >= max_steps:
+                return steps
+
+    # ------------------------------------------------------------------ state
+    def state(self, k: int = 0) -> dict[str, torch.Tensor]:
+        """Raster views (rows x cols) of the latest state of instance k."""
+        cur = self.controls()[k].cur
+        ins = self.inst[k]
+        out = {"h": ins.raster(ins.h[cur]), "qx": ins.raster(ins.qx[cur]),
+               "qy": ins.raster(ins.qy[cur]), "h_max": ins.raster(ins.h_max)}
+        z = ins.raster(ins.z).double().cpu().numpy() + ins.z_abs_offset
+        out["z"] = torch.as_tensor(z)
+        return out
+
+    def compacted(self, k: int = 0) -> dict[str, np.ndarray]:
+        """State of instance k in the reference's compacted (row-major valid) order."""
+        st = self.state(k)
+        v = self.inst[k].valid
+        return {name: (t.cpu().numpy() if torch.is_tensor(t) else t)[v].astype(np.float64)
+                for name, t in st.items()}
+
+    def cell_offsets(self, k: int, rows: np.ndarray, cols: np.ndarray) -> torch.Tensor:
+        """Flat element offsets of raster cells in the dense state arrays (for gather)."""
+        ins = self.inst[k]
+        off = (np.asarray(rows) + _lib.HB_PAD_Y) * ins.pitch + (np.asarray(cols) + _lib.HB_PAD_X)
+        return torch.as_tensor(off.astype(np.int64), device=self.device)
+
+    def current(self, k: int = 0) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
+        cur = self.controls()[k].cur
+        ins = self.inst[k]
+        return ins.h[cur], ins.qx[cur], ins.qy[cur]

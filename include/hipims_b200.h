@@ -1,0 +1,149 @@
+/*
+ * hipims_b200.h -- C ABI of libhipims_b200.so, a B200 (sm_100a) implementation
+ * of the HiPIMS 2-D shallow-water time step.
+ *
+ * Conventions
+ *  - Every function returns 0 on success or a negative HB_ERR_* code;
+ *    hb_last_error() returns a message for the calling thread's last failure.
+ *  - Array arguments are DEVICE pointers owned by the caller (plain pointers
+ *    and sizes, no framework types).  Scalars the reference passes as
+ *    1-element tensors (dx, CFL, t, dt) are device pointers too, so no call
+ *    synchronises with the host.
+ *  - `stream` is a cudaStream_t passed as void*; NULL is the legacy default
+ *    stream.  Work is enqueued asynchronously; errors from the launch are
+ *    reported, errors from kernel execution surface at the next sync.
+ *  - `dtype` is HB_F32 or HB_F64 and applies to every floating array of a call.
+ *
+ * Reference paths below are relative to the reference project root
+ * (HC = CHANS-HiPIMS/hipims/cuda, HP = CHANS-HiPIMS/hipims/pythonHipims).
+ */
+#ifndef HIPIMS_B200_H
+#define HIPIMS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HB_ABI_VERSION 1
+
+enum hb_dtype { HB_F32 = 0, HB_F64 = 1 };
+
+enum hb_status {
+  HB_OK = 0,
+  HB_ERR_ARG = -1,     /* invalid argument (null pointer, bad size, bad dtype) */
+  HB_ERR_CUDA = -2,    /* CUDA runtime error (message in hb_last_error) */
+  HB_ERR_LIMIT = -3,   /* a documented size limit was exceeded */
+  HB_ERR_TIMEOUT = -4  /* a bounded device-side wait gave up */
+};
+
+/* Library identity and last error of the calling thread. */
+int hb_abi_version(void);
+const char *hb_last_error(void);
+/* sizeof of the records in hipims_b200_fused.h, for FFI layout checks:
+ * out[0] = hb_ctrl, out[1] = hb_instance, out[2] = hb_fused_batch. */
+void hb_record_sizes(size_t out[3]);
+
+/* ======================================================================
+ * Compat ops: the reference's torch-extension op surface, one C entry per op.
+ * Same argument meaning, compacted-cell layout and in-place semantics.
+ * ==================================================================== */
+
+/* fluxMask.update(fluxMask, h, index, t)  -- HC/fluxMaskGenerator.cpp:22-29,
+ * kernel HC/fluxMaskGenerator_Kernel.cu:19-42.  out: uint8 (torch.bool) [N]. */
+int hb_flux_mask(int dtype, int64_t N, uint8_t *flux_mask, const void *h,
+                 const int32_t *index, const void *t, void *stream);
+
+/* fluxCal_2ndOrder_jh_improved.addFlux (order = 2,
+ * HC/fluxCal_2ndOrder_jh_improved.cpp:28-53) and
+ * fluxCalculation_jh_modified_surface.addFlux (order = 1,
+ * HC/fluxCal_jh_modified_surface.cpp:28-53).  Accumulates into
+ * h_flux/qx_flux/qy_flux [N] for the M active cells of wet_mask.
+ * Boundary tables are row-major [rows, cols] with time in column 0. */
+int hb_flux(int order, int dtype, int64_t M, int64_t N, const int32_t *wet_mask,
+            void *h_flux, void *qx_flux, void *qy_flux, const void *h,
+            const void *wl, const void *z, const void *qx, const void *qy,
+            const int32_t *index, const void *normal, const void *given_depth,
+            int depth_rows, int depth_cols, const void *given_wl, int wl_rows,
+            int wl_cols, const void *given_q, int q_rows, int q_cols,
+            const void *dx, const void *t, const void *dt, void *stream);
+
+/* friction_implicit_andUpdate_jh.addFriction_eulerUpdate --
+ * HC/friction_implicit_andUpdate_jh_interface.cpp:29-53, kernel
+ * HC/friction_implicit_andUpdate_jh_Kernel.cu:22-146.  landuse: uint8 [N]. */
+int hb_friction_update(int dtype, int64_t M, const int32_t *wet_mask,
+                       void *h_update, void *qx_update, void *qy_update,
+                       void *z_update, const uint8_t *landuse, void *h, void *wl,
+                       void *qx, void *qy, void *z, const void *manning,
+                       const void *dt, void *stream);
+
+/* timeControl.updateTimestep -- HC/timeControl.cpp:27-41, kernel
+ * HC/timeControl_Kernel.cu:164-198.  accelerator [M] out, h_max [N] in/out. */
+int hb_timestep(int dtype, int64_t M, const int32_t *wet_mask, void *accelerator,
+                void *h_max, const void *h, const void *qx, const void *qy,
+                const void *dx, const void *cfl, const void *t, const void *dt,
+                void *stream);
+
+/* station_PrecipitationCalculation.addStation_Precipitation --
+ * HC/stationPrecipitation_interface.cpp:26-38, kernel
+ * HC/stationPrecipitation_Kernel.cu:18-29.  mask: int16 [N]. */
+int hb_rain_station(int dtype, int64_t N, void *h_update, const int16_t *mask,
+                    const void *station_data, const void *dt, void *stream);
+
+/* euler_update.update -- HC/euler_update.cpp:27-44, kernel
+ * HC/euler_update_Kernel.cu:18-36. */
+int hb_euler_update(int dtype, int64_t M, const int32_t *update_mask,
+                    const void *h_update, const void *qx_update,
+                    const void *qy_update, const void *z_update, void *h,
+                    void *wl, void *z, void *qx, void *qy, void *stream);
+
+/* infiltrationCalculation.addinfiltration -- HC/infiltration_interface.cpp,
+ * kernel HC/infiltrationCUDA_Kernel.cu:20-46 (Green-Ampt). */
+int hb_infiltration(int dtype, int64_t M, const int32_t *wet_mask, void *h_update,
+                    const uint8_t *landuse, const void *h, const void *ks,
+                    const void *psi, const void *dtheta, void *cumulative,
+                    const void *dt, void *stream);
+
+/* Device-side minimum of x[0..M) written to out[0] -- replaces the
+ * torch.min(accelerator) of HP/SWE_CUDA.py:818-820 without a host sync.
+ * workspace: hb_min_reduce_workspace_size(M) bytes, or NULL when M <= 4096. */
+size_t hb_min_reduce_workspace_size(int64_t M);
+int hb_min_reduce(int dtype, int64_t M, const void *x, void *out, void *workspace,
+                  void *stream);
+
+/* ======================================================================
+ * Fused dense-tile step (no reference counterpart; replaces the sequence
+ * addFlux -> rain -> friction/update -> timeControl -> min of
+ * HP/SWE_CUDA.py:339-424, 497-502, 780-831 with one kernel per step).
+ * A batch of instances (catchments) advances together; a single run is a
+ * batch of one.  Layout and argument records are defined in
+ * hipims_b200_fused.h.
+ * ==================================================================== */
+struct hb_fused_batch; /* host-side launch record, see hipims_b200_fused.h */
+
+/* Bytes of device workspace one step needs (per-tile partial sums). */
+size_t hb_fused_workspace_size(const struct hb_fused_batch *batch);
+/* Initialise the control blocks: rain rate and boundary values at t, zero
+ * counters.  Call once before the first step and after host edits of ctrl. */
+int hb_fused_prepare(const struct hb_fused_batch *batch, void *stream);
+/* Enqueue `nsteps` fused steps (graph-capturable; no host sync). */
+int hb_fused_step(const struct hb_fused_batch *batch, int nsteps, void *stream);
+
+/* ======================================================================
+ * Coupling gather (no reference counterpart; replaces the
+ * h[idx_target_ABM1] gather of CHANS-HiPIMS/CHANS-HiPIMS_server.py:255-256).
+ * Gathers depth (and optionally velocities u = qx/h, v = qy/h, 0 when dry)
+ * at n agent cells given as flat raster offsets (row * pitch + col of the
+ * dense arrays).  out: float [n] per requested field.
+ * ==================================================================== */
+int hb_gather(int dtype, int64_t n, const int64_t *cell_offsets, const void *h,
+              const void *qx, const void *qy, void *out_h, void *out_u,
+              void *out_v, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HIPIMS_B200_H */

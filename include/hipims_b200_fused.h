@@ -1,0 +1,112 @@
+/*
+ * hipims_b200_fused.h -- records of the fused dense-tile step (hb_fused_*).
+ *
+ * Dense layout (one instance = one catchment raster of rows x cols cells):
+ *  - State arrays (h, qx, qy, z, h_max) are row-major with `pitch` elements
+ *    per row.  Raster cell (r, c) lives at element (r + 2) * pitch + (c + 4):
+ *    two halo rows above, four columns on the left so that every tile load,
+ *    halo included, starts on a 16-byte boundary.  Storage has at least
+ *    round_up(rows, 64) + 4 rows and pitch >= round_up(cols, 64) + 8.
+ *  - The cell code array (uint8) has `code_pitch` bytes per row, raster
+ *    cell (r, c) at (r + 2) * code_pitch + (c + 16).  Low nibble = Manning
+ *    zone, high nibble = boundary class; class 15 = no-data.  Padding is
+ *    no-data (0xF0).
+ *  - In FP32 mode z is stored relative to a datum per 64 x 64 block of the
+ *    raster (datum[by * datum_nx + bx], integer-valued floats), so that
+ *    eta = h + z keeps sub-millimetre resolution on high terrain.  FP64 mode
+ *    stores z absolute with a zero datum.
+ *  - State buffers ping-pong: ctrl->cur names the one holding the latest
+ *    state; a step reads cur and writes 1 - cur.
+ */
+#ifndef HIPIMS_B200_FUSED_H
+#define HIPIMS_B200_FUSED_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HB_MAX_CLASSES 16
+#define HB_NODATA_CLASS 15
+#define HB_MAX_ZONES 16
+#define HB_DATUM_BLOCK 64
+#define HB_PAD_Y 2
+#define HB_PAD_X 4
+#define HB_CODE_PAD_X 16
+
+/* Per-instance control block, device memory.  Written by hb_fused_prepare
+ * and by the last tile of every step; read by the host between launches. */
+typedef struct hb_ctrl {
+  double t;              /* simulated time of the next step (HP/SWE_CUDA.py self.t) */
+  double dt;             /* time step of the next step (self.dt) */
+  double export_step;    /* Export_timeStep; dt is clipped to its multiples */
+  double t_end;          /* the step that reaches t >= t_end halts the instance */
+  double volume;         /* FP64 sum of h * dx^2 over valid cells, after the last step */
+  double volume0;        /* volume at prepare */
+  double rain_volume;    /* FP64 accumulated rain input (m^3) */
+  double outflow_volume; /* FP64 accumulated boundary outflow (m^3) */
+  double rain_rate;      /* uniform rain rate (m/s) used by the next step */
+  double rain_mult;      /* multiplier applied to the rain table */
+  int64_t step;          /* steps taken */
+  int32_t export_n;      /* export counter (self._export_n) */
+  int32_t cur;           /* state buffer holding the latest state */
+  int32_t halted;        /* nonzero: steps are no-ops */
+  int32_t halt_on_export;/* nonzero: halt after a step that hits an export time */
+  int32_t exports;       /* export clips taken */
+  int32_t rain_index;    /* monotone cursor into the rain table */
+  uint32_t tiles_done;   /* internal last-tile-done counter */
+  int32_t status;        /* nonzero: a NaN/inf was seen in dt */
+  float bc_vals[HB_MAX_CLASSES][4]; /* given h, wl, qx, qy per class at t */
+} hb_ctrl;
+
+/* One catchment.  Pointers are device pointers. */
+typedef struct hb_instance {
+  int32_t rows, cols;        /* raster size */
+  int32_t tiles_x, tiles_y;  /* tile grid over the raster */
+  int32_t tile_begin;        /* first flat tile index of this instance */
+  int32_t pitch;             /* elements per row of the state arrays */
+  int32_t code_pitch;        /* bytes per row of the code array */
+  int32_t datum_nx, datum_ny;/* datum blocks */
+  int32_t bug_y, bug_x;      /* raster cell whose compacted id is 0, or -1 */
+  int32_t rain_rows, rain_cols;
+  int32_t depth_rows, depth_cols, wl_rows, wl_cols, q_rows, q_cols;
+  int32_t pad0;
+  void *h[2], *qx[2], *qy[2];/* ping-pong state */
+  void *z;                   /* bed elevation (datum-relative in FP32 mode) */
+  void *h_max;               /* running maximum depth */
+  const uint8_t *code;       /* zone | class << 4 */
+  const float *datum;        /* [datum_ny * datum_nx] */
+  hb_ctrl *ctrl;
+  const double *rain_tab;    /* [rain_rows, rain_cols]: time, rate (m/s) */
+  const double *given_depth; /* boundary tables, HP/SWE_CUDA.py:102-110 layout */
+  const double *given_wl;
+  const double *given_q;
+  double dx, cfl;
+  double manning[HB_MAX_ZONES];
+  int32_t bc_type[HB_MAX_CLASSES]; /* 1 interior, 3..8 ghost types */
+  int32_t bc_id[HB_MAX_CLASSES];
+  int64_t n_valid;           /* valid cells */
+  const double *dt_replay;   /* optional: dt of step k+1 is dt_replay[k] for k < n_replay */
+  int64_t n_replay;          /* (frozen time-step schedule; 0 = adaptive CFL step) */
+} hb_instance;
+
+/* Launch record (host memory). */
+typedef struct hb_fused_batch {
+  int32_t dtype;             /* HB_F32 or HB_F64 */
+  int32_t n_instances;
+  int32_t n_tiles;           /* sum of tiles_x * tiles_y */
+  int32_t tile_y, tile_x;    /* tile shape: 8, 16, 32 or 64 each */
+  int32_t grid_blocks;       /* 0: one wave of resident blocks */
+  int32_t order;             /* 2 (MUSCL); 1 (bed-only minmod) */
+  int32_t flags;             /* reserved, 0 */
+  const hb_instance *instances;  /* device [n_instances] */
+  const int32_t *tile_instance;  /* device [n_tiles] */
+  void *workspace;               /* device, hb_fused_workspace_size() bytes */
+} hb_fused_batch;
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HIPIMS_B200_FUSED_H */

@@ -1,0 +1,127 @@
+"""Generate the golden fixtures of tests/golden/ from the reference's own kernels.
+
+Runs the reference's HiPIMS kernels compiled for the host (oracle/_ref, built
+from the reference sources by oracle/build_ref.py) under the reference's step
+order, on small seeded cases, and stores inputs and outputs as .npz.  The
+fixtures pin the CPU restatement (oracle/hipims_oracle.c) where oracle/_ref is
+not available, e.g. on a machine without the reference tree.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "chans-hipims-flamegpu_b200"))
+
+from hipims_b200 import scenarios as S  # noqa: E402
+from hipims_b200.topology import boundary_codes  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+KEYS = ("mask", "z", "h", "qx", "qy", "wl", "landuse", "rain_mask")
+
+
+def mixed_bc_case(seed: int, order: int) -> dict:
+    """20 x 24 valid cells, bumpy bed, wet/dry mix, every boundary type."""
+    rng = np.random.default_rng(seed)
+    ny, nx = 20, 24
+    nodata = np.zeros((ny + 2, nx + 2), dtype=bool)
+    nodata[0, :] = nodata[-1, :] = nodata[:, 0] = nodata[:, -1] = True
+    nodata[8:11, 10:13] = True  # an interior hole
+    types = [3, 4, 6, 7, 8] + ([9] if order == 1 else [])
+    boxes = [(0, ny + 2, 0, 2, 6), (0, ny + 2, nx, nx + 2, 5), (0, 2, 2, 9, 3),
+             (0, 2, 9, 16, 7), (ny, ny + 2, 2, 12, 8), (ny, ny + 2, 12, nx, 4)]
+    if order == 1:
+        boxes.append((0, 2, 16, nx, 9))
+    mask = boundary_codes(nodata, default_bc=50, boxes=boxes)
+    z = rng.uniform(0.0, 0.3, mask.shape) + np.linspace(0.0, 0.2, mask.shape[1])[None, :]
+    h = np.where(rng.uniform(size=mask.shape) < 0.7, rng.uniform(0.0, 0.4, mask.shape), 0.0)
+    h[:, : mask.shape[1] // 3] += 0.3
+    qx = rng.normal(0.0, 0.05, mask.shape) * (h > 0)
+    qy = rng.normal(0.0, 0.05, mask.shape) * (h > 0)
+    h[nodata] = qx[nodata] = qy[nodata] = 0.0
+    landuse = (rng.uniform(size=mask.shape) < 0.4).astype(np.uint8)
+    rain_mask = (rng.uniform(size=mask.shape) < 0.5).astype(np.int16)
+    return dict(mask=mask, z=z, h=h, qx=qx, qy=qy, wl=z + h, landuse=landuse,
+                rain_mask=rain_mask, manning=[0.02, 0.05], dx=0.5, cfl=0.5, first_dt=1.0e-3,
+                rain=np.array([[0.0, 1e-4, 2e-4], [1.0, 3e-4, 0.0], [5.0, 0.0, 1e-4]]),
+                given_depth=np.array([[0.0, 0.3], [0.5, 0.45], [100.0, 0.2]]),
+                given_wl=np.array([[0.0, 0.6], [100.0, 0.7]]),
+                given_q=np.array([[0.0, 0.05, 0.01], [1.0, 0.1, -0.02], [100.0, 0.0, 0.0]]),
+                export_step=0.75, steps=60, types=np.array(types))
+
+
+def cases() -> dict:
+    out = {}
+    d = S.dam_break(48)
+    d.update(steps=120)
+    out["dam_break48_o2"] = (d, 2)
+    out["dam_break48_o1"] = (dict(d), 1)
+    c = S.channel()
+    c.update(steps=100000)
+    out["channel_o2"] = (c, 2)
+    c1 = dict(c)
+    c1["t_end"] = 2.0
+    out["channel_o1"] = (c1, 1)
+    out["mixed_bc_o2"] = (mixed_bc_case(11, 2), 2)
+    out["mixed_bc_o1"] = (mixed_bc_case(12, 1), 1)
+    return out
+
+
+def run_case(d: dict, order: int, backend: str) -> tuple[dict, int]:
+    sim = O.Sim(d, order=order, backend=backend, export_step=d.get("export_step", 1.0e30))
+    n = sim.run(int(d["steps"]), float(d.get("t_end", np.inf)))
+    st = sim.state()
+    st["steps"] = n
+    st["exports"] = sim.g.exports
+    return st, n
+
+
+def main() -> None:
+    if not O.ref_available():
+        raise SystemExit("oracle/_ref is not built: python oracle/build_ref.py")
+    for name, (d, order) in cases().items():
+        st, n = run_case(d, order, "ref")
+        payload = {k: np.asarray(d[k]) for k in KEYS if d.get(k) is not None}
+        for k in ("manning", "rain", "given_depth", "given_wl", "given_q"):
+            if d.get(k) is not None:
+                payload[k] = np.asarray(d[k], dtype=np.float64)
+        scal = dict(dx=d["dx"], cfl=d["cfl"], first_dt=d["first_dt"], order=order,
+                    steps=d["steps"], t_end=d.get("t_end", np.inf),
+                    export_step=d.get("export_step", 1.0e30))
+        for k, v in scal.items():
+            payload["in_" + k] = np.asarray(v, dtype=np.float64)
+        for k in ("h", "qx", "qy", "wl", "h_max"):
+            payload["out_" + k] = st[k]
+        payload["out_t"] = np.asarray(st["t"])
+        payload["out_dt"] = np.asarray(st["dt"])
+        payload["out_steps"] = np.asarray(n)
+        payload["out_exports"] = np.asarray(st["exports"])
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, **payload)
+        print(f"{name}: {n} steps, t={st['t']:.6f}, -> {os.path.getsize(path)} bytes")
+
+
+def load_case(path: str) -> tuple[dict, int, dict]:
+    """Inverse of main(): (inputs dict for oracle.Sim, order, expected outputs)."""
+    z = np.load(path)
+    d = {k: z[k] for k in KEYS if k in z.files}
+    for k in ("manning", "rain", "given_depth", "given_wl", "given_q"):
+        if k in z.files:
+            d[k] = z[k]
+    for k in ("dx", "cfl", "first_dt", "steps", "t_end", "export_step"):
+        d[k] = float(z["in_" + k])
+    d["steps"] = int(d["steps"])
+    order = int(z["in_order"])
+    exp = {k[4:]: z[k] for k in z.files if k.startswith("out_")}
+    return d, order, exp
+
+
+if __name__ == "__main__":
+    main()

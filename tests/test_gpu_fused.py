@@ -1,0 +1,187 @@
+"""Fused dense-tile step against the oracle.
+
+FP64 fused: every face is evaluated once from its west/south cell, which is
+exact up to the HLLC solver's round-off asymmetry, so the tolerance is 1e-10 m.
+FP32 fused: compared with the FP64 oracle at identical simulated times (the
+oracle's dt sequence is replayed) with the north-star tolerance, max depth
+error <= 1e-4 m; the adaptive FP32 run is checked too."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+import make_golden as G
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def catchment(d, **over):
+    from hipims_b200.scenarios import catchment_from
+
+    return catchment_from(d, **over)
+
+
+def compare(fs, sim, k=0):
+    got = fs.compacted(k)
+    st = sim.state()
+    return {f: float(np.abs(got[f] - st[f]).max()) for f in ("h", "qx", "qy", "h_max")}
+
+
+@pytest.mark.parametrize("tile", [(32, 32), (16, 32)])
+def test_fused_fp64_dam_break(cuda, tile):
+    from hipims_b200 import scenarios as S
+    from hipims_b200.fused import FusedSolver
+
+    d = S.dam_break(100)
+    sim = O.Sim(d, order=2)
+    sim.run(300)
+    fs = FusedSolver(catchment(d), dtype=torch.float64, tile=tile, device=cuda)
+    fs.step(300)
+    c = fs.controls()[0]
+    assert c.step == 300
+    assert c.t == pytest.approx(sim.t, rel=1e-12)
+    err = compare(fs, sim)
+    assert max(err.values()) < 1e-10, err
+
+
+def test_fused_fp64_channel_boundaries(cuda):
+    """H_GIVEN inflow, OPEN outflow, walls: the back-channel case to t = 8 s."""
+    from hipims_b200 import scenarios as S
+    from hipims_b200.fused import FusedSolver
+
+    d = S.channel()
+    sim = O.Sim(d, order=2)
+    n = sim.run(100000, d["t_end"])
+    fs = FusedSolver(catchment(d, t_end=d["t_end"]), dtype=torch.float64, device=cuda)
+    fs.step(n + 5)
+    c = fs.controls()[0]
+    assert c.step == n and c.halted
+    err = compare(fs, sim)
+    assert max(err.values()) < 1e-10, err
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_fused_fp64_mixed_boundaries_uniform_rain(cuda, seed):
+    from hipims_b200.fused import FusedSolver
+
+    d = G.mixed_bc_case(200 + seed, 2)
+    d.pop("rain_mask")
+    d["rain"] = np.array([[0.0, 2e-4], [1.0, 5e-4], [10.0, 0.0]])
+    sim = O.Sim(d, order=2, export_step=0.75)
+    sim.run(60)
+    fs = FusedSolver(catchment(d, export_step=0.75), dtype=torch.float64, device=cuda)
+    fs.step(60)
+    c = fs.controls()[0]
+    assert c.exports == sim.g.exports and c.t == pytest.approx(sim.t, rel=1e-12)
+    err = compare(fs, sim)
+    assert max(err.values()) < 1e-10, err
+
+
+def test_fused_fp32_dam_break_1000_steps(cuda):
+    """Config 1 (256 x 256, 1000 steps) in FP32 vs the FP64 oracle."""
+    from hipims_b200 import scenarios as S
+    from hipims_b200.fused import FusedSolver
+
+    d = S.dam_break(256)
+    sim = O.Sim(d, order=2)
+    dts = sim.run_record(1000)
+    fs = FusedSolver(catchment(d, dt_replay=dts), dtype=torch.float32, device=cuda)
+    fs.step(1000)
+    err = compare(fs, sim)
+    print("FP32 fused vs FP64 oracle (replayed dt), 1000 steps:", err)
+    assert err["h"] <= 1e-4
+    # adaptive FP32 dt stays within round-off of the FP64 schedule
+    fa = FusedSolver(catchment(d), dtype=torch.float32, device=cuda)
+    fa.step(1000)
+    assert fa.controls()[0].t == pytest.approx(sim.t, rel=1e-4)
+
+
+def test_fused_fp32_urban_rain(cuda):
+    """Config-2 physics on a 192 x 192 catchment: DEM with buildings, two
+    Manning zones, open ring, dry start, 50 mm/h rain."""
+    from hipims_b200 import scenarios as S
+    from hipims_b200.fused import FusedSolver
+
+    d = S.urban_catchment(192, dx=2.0, seed=3, rain_mm_h=200.0)
+    sim = O.Sim(d, order=2)
+    dts = sim.run_record(400)
+    fs = FusedSolver(catchment(d, dt_replay=dts), dtype=torch.float32, device=cuda)
+    fs.step(400)
+    err = compare(fs, sim)
+    print("urban FP32 vs FP64 oracle:", err, "t", sim.t, "hmax", sim.h.max())
+    assert err["h"] <= 1e-4
+
+
+def test_fused_batch_equals_single_runs(cuda):
+    from hipims_b200 import scenarios as S
+    from hipims_b200.fused import FusedSolver
+
+    ds = [S.urban_catchment(n, seed=k, rain_mm_h=100.0) for k, n in enumerate((70, 130, 96))]
+    cs = [catchment(d) for d in ds]
+    fb = FusedSolver(cs, dtype=torch.float32, device=cuda)
+    fb.step(50)
+    for k, c in enumerate(cs):
+        f1 = FusedSolver(c, dtype=torch.float32, device=cuda)
+        f1.step(50)
+        a, b = fb.compacted(k), f1.compacted(0)
+        for f in ("h", "qx", "qy"):
+            np.testing.assert_array_equal(a[f], b[f])
+        assert fb.controls()[k].t == f1.controls()[0].t
+
+
+def test_fused_graph_replay_equals_eager(cuda):
+    from hipims_b200 import scenarios as S
+    from hipims_b200.fused import FusedSolver
+
+    d = S.urban_catchment(120, seed=9, rain_mm_h=100.0)
+    a = FusedSolver(catchment(d), dtype=torch.float32, device=cuda)
+    b = FusedSolver(catchment(d), dtype=torch.float32, device=cuda)
+    a.step(40)
+    b.capture(10)
+    for _ in range(4):
+        b.replay()
+    torch.cuda.synchronize()
+    for f in ("h", "qx", "qy"):
+        np.testing.assert_array_equal(a.compacted()[f], b.compacted()[f])
+
+
+def test_fused_export_halt_and_resume(cuda):
+    from hipims_b200 import scenarios as S
+    from hipims_b200.fused import FusedSolver
+
+    d = S.dam_break(64)
+    fs = FusedSolver(catchment(d, export_step=2.0, halt_on_export=True), dtype=torch.float32,
+                     device=cuda)
+    fs.step(500)
+    c = fs.controls()[0]
+    assert c.halted and c.exports == 1 and c.t == 2.0
+    steps = c.step
+    fs.step(10)
+    assert fs.controls()[0].step == steps  # halted steps are no-ops
+    fs.resume()
+    fs.step(500)
+    c = fs.controls()[0]
+    assert c.exports == 2 and c.t == 4.0
+
+
+def test_fused_mass_balance(cuda):
+    """Closed box with rain: V - V0 = rain; open catchment: V - V0 = rain - outflow."""
+    from hipims_b200 import scenarios as S
+    from hipims_b200.fused import FusedSolver
+
+    d = S.dam_break(64, ring_code=30)
+    d["rain"] = np.array([[0.0, 1e-3], [1e6, 1e-3]])
+    fs = FusedSolver(catchment(d), dtype=torch.float32, device=cuda)
+    fs.step(200)
+    c = fs.controls()[0]
+    rel = abs(c.volume - c.volume0 - c.rain_volume) / c.rain_volume
+    assert rel < 1e-5, rel
+    u = S.urban_catchment(128, seed=4, rain_mm_h=500.0)
+    fo = FusedSolver(catchment(u), dtype=torch.float32, device=cuda)
+    fo.step(600)
+    c = fo.controls()[0]
+    assert c.outflow_volume > 0
+    rel = abs(c.volume - c.volume0 - c.rain_volume + c.outflow_volume) / c.rain_volume
+    assert rel < 1e-4, rel

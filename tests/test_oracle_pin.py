@@ -1,0 +1,135 @@
+"""Pin the CPU oracle: the restatement must reproduce the reference's own
+kernels (compiled for the host) bit for bit, on the committed golden fixtures
+and, when oracle/_ref is built, on fresh cases."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import make_golden as G
+from oracle import oracle as O
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+FIELDS = ("h", "qx", "qy", "wl", "h_max")
+
+
+def test_golden_fixtures_exist():
+    names = {os.path.basename(p) for p in GOLDEN}
+    for n in ("dam_break48_o2.npz", "channel_o2.npz", "mixed_bc_o2.npz", "mixed_bc_o1.npz"):
+        assert n in names
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_oracle_matches_golden(path):
+    d, order, exp = G.load_case(path)
+    sim = O.Sim(d, order=order, backend="oracle", export_step=d["export_step"])
+    n = sim.run(d["steps"], d["t_end"])
+    st = sim.state()
+    assert n == int(exp["steps"])
+    assert st["t"] == float(exp["t"]) and st["dt"] == float(exp["dt"])
+    assert sim.g.exports == int(exp["exports"])
+    for k in FIELDS:
+        np.testing.assert_array_equal(st[k], exp[k], err_msg=k)
+
+
+needs_ref = pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built")
+
+
+@needs_ref
+@pytest.mark.parametrize("order", [1, 2])
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_oracle_matches_reference_build(order, seed):
+    d = G.mixed_bc_case(100 + seed, order)
+    a = O.Sim(d, order=order, backend="oracle", export_step=d["export_step"])
+    b = O.Sim(d, order=order, backend="ref", export_step=d["export_step"])
+    a.run(40)
+    b.run(40)
+    sa, sb = a.state(), b.state()
+    assert sa["t"] == sb["t"]
+    for k in FIELDS:
+        np.testing.assert_array_equal(sa[k], sb[k], err_msg=k)
+
+
+@needs_ref
+def test_single_kernels_match_reference_build():
+    """Each kernel alone, on one random state, against the reference kernel."""
+    import ctypes
+
+    d = G.mixed_bc_case(7, 2)
+    a = O.Sim(d, order=2)
+    R = O.ref_lib()
+    N = a.N
+    rng = np.random.default_rng(0)
+    wet = np.arange(N, dtype=np.int32)
+    for order, sym in ((2, "ref_flux2"), (1, "ref_flux1")):
+        out_o = [np.zeros(N) for _ in range(3)]
+        out_r = [np.zeros(N) for _ in range(3)]
+        O.flux(order, wet, *out_o, a.h, a.wl, a.z, a.qx, a.qy, a.index, a.normal, a.gd, a.gw,
+               a.gq, 0.5, 0.3, 0.01)
+        dx, t, dt = (ctypes.c_double(v) for v in (0.5, 0.3, 0.01))
+        P = lambda x: x.ctypes.data
+        getattr(R, sym)(N, N, a.gd.shape[1], a.gd.shape[0], a.gw.shape[1], a.gw.shape[0],
+                        a.gq.shape[1], a.gq.shape[0], ctypes.c_void_p(P(wet)),
+                        *(ctypes.c_void_p(P(x)) for x in (a.h, a.wl, a.z, a.qx, a.qy, a.index,
+                                                          a.normal, a.gd, a.gw, a.gq)),
+                        ctypes.byref(dx), ctypes.byref(t), ctypes.byref(dt),
+                        *(ctypes.c_void_p(P(x)) for x in out_r))
+        for x, y in zip(out_o, out_r):
+            np.testing.assert_array_equal(x, y)
+    assert rng is not None
+
+
+def test_topology_pin_backcase():
+    """HP/backCase.ipynb prints torch.Size([5, 5625]) for its 27 x 227 raster."""
+    from hipims_b200 import scenarios as S
+
+    c = S.channel()
+    assert c["mask"].shape == (27, 227)
+    idx = O.build_index(c["mask"].astype(np.int32))
+    assert idx.size == 5 * 5625
+
+
+def test_physics_lake_at_rest():
+    """Flat free surface over a bumpy bed, closed walls: stays at rest."""
+    from hipims_b200 import scenarios as S
+
+    d = S.dam_break(32, ring_code=30)
+    rng = np.random.default_rng(3)
+    z = rng.uniform(0.0, 0.5, d["mask"].shape)
+    d["z"] = z
+    d["h"] = np.where(d["mask"] > 0, 1.0 - z, 0.0)
+    d["wl"] = d["z"] + d["h"]
+    sim = O.Sim(d, order=2)
+    sim.run(200)
+    st = sim.state()
+    assert np.abs(st["qx"]).max() < 1e-12 and np.abs(st["qy"]).max() < 1e-12
+    assert np.abs(st["h"] + sim.z - 1.0).max() < 1e-12
+
+
+def test_physics_mass_conservation_walls():
+    from hipims_b200 import scenarios as S
+
+    d = S.dam_break(32, ring_code=40)
+    sim = O.Sim(d, order=2)
+    v0 = sim.h.sum()
+    sim.run(300)
+    assert abs(sim.h.sum() - v0) / v0 < 1e-12
+
+
+def test_physics_rain_in_closed_box():
+    from hipims_b200 import scenarios as S
+
+    d = S.dam_break(16, ring_code=30)
+    d["h"] = np.where(d["mask"] > 0, 0.1, 0.0)
+    d["rain"] = np.array([[0.0, 1e-3], [1000.0, 1e-3]])
+    d["rain_mask"] = np.zeros(d["mask"].shape, np.int16)
+    sim = O.Sim(d, order=2)
+    v0 = sim.h.sum()
+    t0 = sim.t
+    total = 0.0
+    for _ in range(50):
+        total += 1e-3 * sim.dt * sim.N
+        sim.step()
+    assert abs((sim.h.sum() - v0) - total) / total < 1e-10
+    assert sim.t > t0
