@@ -78,10 +78,12 @@ flux_kernel(int64_t M, int64_t N, const int32_t *__restrict__ wet,
     if (r_id == -1) {
       int bt, bid;
       decode_bc(c_type, bt, bid);
-      T hb = gd[(int64_t)tl_d * dc + bid + 1];
-      T wlb = gw[(int64_t)tl_w * wc + bid + 1];
-      T qxb = gq[(int64_t)tl_q * qc + 1 + 2 * bid];
-      T qyb = gq[(int64_t)tl_q * qc + 2 + 2 * bid];
+      // Table columns beyond the given width read as 0 (the reference reads
+      // past the row there).
+      T hb = bid + 1 < dc ? gd[(int64_t)tl_d * dc + bid + 1] : T(0);
+      T wlb = bid + 1 < wc ? gw[(int64_t)tl_w * wc + bid + 1] : T(0);
+      T qxb = 2 + 2 * bid < qc ? gq[(int64_t)tl_q * qc + 1 + 2 * bid] : T(0);
+      T qyb = 2 + 2 * bid < qc ? gq[(int64_t)tl_q * qc + 2 + 2 * bid] : T(0);
       if (!ghost(bt, ORDER == 1, c, n0, n1, hb, wlb, qxb, qyb, r)) continue;
       r_h = r.h;
       r_z = r.z;

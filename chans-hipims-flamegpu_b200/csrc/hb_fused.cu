@@ -190,8 +190,8 @@ __device__ double rain_rate_at(const hb_instance &in, hb_ctrl *c, double t) {
   const double *R = in.rain_tab;
   const int C = in.rain_cols;
   if (!(t < R[(int64_t)(in.rain_rows - 1) * C])) return 0.0;
-  int idx = c->rain_index;
-  while (!(t < R[(int64_t)(idx + 1) * C])) idx++;
+  int idx = min(max(c->rain_index, 0), in.rain_rows - 2);
+  while (idx + 2 < in.rain_rows && !(t < R[(int64_t)(idx + 1) * C])) idx++;
   c->rain_index = idx;
   const double *r0 = R + (int64_t)idx * C, *r1 = r0 + C;
   const double per = (t - r0[0]) / (r1[0] - r0[0]);
