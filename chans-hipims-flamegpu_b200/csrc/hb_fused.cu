@@ -262,11 +262,10 @@ inline size_t ws_partials_bytes(int n_tiles) {
 // ---------------------------------------------------------------------------
 // The step kernel
 // ---------------------------------------------------------------------------
-template <typename T, int TY, int TX>
+template <typename T, int TY, int TX, bool FAST>
 __global__ void __launch_bounds__(kNT)
 fused_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restrict__ tile_inst,
                   int n_tiles, TilePartial *__restrict__ partials, BcTable *__restrict__ bct) {
-  constexpr bool FAST = (sizeof(T) == 4);
   using S = Smem<T, TY, TX>;
   constexpr int SW = S::SW, SH = S::SH;
   constexpr int V = 16 / sizeof(T);  // elements per 16-byte vector
@@ -476,7 +475,9 @@ fused_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restri
         const T n = (T)in.manning[code & 15];
         qx += qxu;
         qy += qyu;
-        sgh = (T)sqrtf((float)(g * h));
+        // the reference takes this square root in single precision
+        // (HC/timeControl_Kernel.cu:188); FAST allows the approximate one
+        sgh = FAST ? (T)sqrtf((float)(g * h)) : (T)__fsqrt_rn((float)(g * h));
         if constexpr (FAST) {
           if (n > T(0)) {
             const T ih = T(1) / h;
@@ -684,18 +685,18 @@ prepare_kernel(const hb_instance *__restrict__ insts, BcTable *__restrict__ bct)
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
-template <typename T, int TY, int TX>
+template <typename T, int TY, int TX, bool FAST = (sizeof(T) == 4)>
 int launch_steps(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   using S = Smem<T, TY, TX>;
   static std::once_flag once;
   static cudaError_t attr_err = cudaSuccess;
   static int blocks_per_sm = 1;
   std::call_once(once, [] {
-    attr_err = cudaFuncSetAttribute(fused_step_kernel<T, TY, TX>,
+    attr_err = cudaFuncSetAttribute(fused_step_kernel<T, TY, TX, FAST>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(S));
     if (attr_err == cudaSuccess)
       attr_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &blocks_per_sm, fused_step_kernel<T, TY, TX>, kNT, sizeof(S));
+          &blocks_per_sm, fused_step_kernel<T, TY, TX, FAST>, kNT, sizeof(S));
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   });
   if (attr_err != cudaSuccess)
@@ -705,7 +706,7 @@ int launch_steps(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   TilePartial *parts = reinterpret_cast<TilePartial *>(b->workspace);
   BcTable *bct = reinterpret_cast<BcTable *>((char *)b->workspace + ws_partials_bytes(b->n_tiles));
   for (int k = 0; k < nsteps; k++) {
-    fused_step_kernel<T, TY, TX><<<grid, kNT, sizeof(S), st>>>(b->instances, b->tile_instance,
+    fused_step_kernel<T, TY, TX, FAST><<<grid, kNT, sizeof(S), st>>>(b->instances, b->tile_instance,
                                                                 b->n_tiles, parts, bct);
   }
   return check_launch("hb_fused_step");
@@ -743,6 +744,10 @@ extern "C" int hb_fused_step(const hb_fused_batch *b, int nsteps, void *stream) 
   if (nsteps == 0) return HB_OK;
   auto st = as_stream(stream);
   const int ty = b->tile_y, tx = b->tile_x;
+  if (b->dtype == HB_F32 && (b->flags & HB_FLAG_EXACT_FP32)) {
+    if (ty == 32 && tx == 32) return launch_steps<float, 32, 32, false>(b, nsteps, st);
+    return set_error(HB_ERR_ARG, "hb_fused_step: exact FP32 tile %dx%d not built", ty, tx);
+  }
   if (b->dtype == HB_F32) {
     if (ty == 32 && tx == 32) return launch_steps<float, 32, 32>(b, nsteps, st);
     if (ty == 16 && tx == 64) return launch_steps<float, 16, 64>(b, nsteps, st);

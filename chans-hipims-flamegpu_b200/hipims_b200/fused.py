@@ -167,7 +167,8 @@ class FusedSolver:
     """Advance one or more catchments with the fused dense-tile kernel."""
 
     def __init__(self, catchments: Catchment | Sequence[Catchment], dtype=torch.float32,
-                 tile: tuple[int, int] = (32, 32), device="cuda", grid_blocks: int = 0):
+                 tile: tuple[int, int] = (32, 32), device="cuda", grid_blocks: int = 0,
+                 exact_fp32: bool = False):
         if isinstance(catchments, Catchment):
             catchments = [catchments]
         if dtype not in (torch.float32, torch.float64):
@@ -239,6 +240,7 @@ class FusedSolver:
         b.tile_y, b.tile_x = self.tile
         b.grid_blocks = grid_blocks
         b.order = 2
+        b.flags = 1 if exact_fp32 else 0
         b.instances = self.records.data_ptr()
         b.tile_instance = self.tile_instance.data_ptr()
         L = _lib.lib()

@@ -34,6 +34,9 @@ extern "C" {
 #define HB_PAD_Y 2
 #define HB_PAD_X 4
 #define HB_CODE_PAD_X 16
+/* hb_fused_batch.flags: FP32 with the reference's operation forms (no
+ * approximate division/square root, no algebraic shortcuts). */
+#define HB_FLAG_EXACT_FP32 1
 
 /* Per-instance control block, device memory.  Written by hb_fused_prepare
  * and by the last tile of every step; read by the host between launches. */
@@ -99,7 +102,7 @@ typedef struct hb_fused_batch {
   int32_t tile_y, tile_x;    /* tile shape: 8, 16, 32 or 64 each */
   int32_t grid_blocks;       /* 0: one wave of resident blocks */
   int32_t order;             /* 2 (MUSCL); 1 (bed-only minmod) */
-  int32_t flags;             /* reserved, 0 */
+  int32_t flags;             /* HB_FLAG_* bits */
   const hb_instance *instances;  /* device [n_instances] */
   const int32_t *tile_instance;  /* device [n_tiles] */
   void *workspace;               /* device, hb_fused_workspace_size() bytes */
