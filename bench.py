@@ -249,7 +249,7 @@ def run_ours(args) -> None:
                                                      "sim_time_s": c.t, "dt_s": c.dt}),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
-                         "kernel": "fused_step_kernel<float,32,32>",
+                         "kernel": f"rows_step_kernel<float,{args.tile[0]}>",
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "traffic": profiled_traffic()},
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": bytes_io,
@@ -305,7 +305,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cells", type=int, default=N_CELLS)
-    ap.add_argument("--tile", type=int, nargs=2, default=[32, 32])
+    ap.add_argument("--tile", type=int, nargs=2, default=[64, 32])
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-accuracy", dest="accuracy", action="store_false")

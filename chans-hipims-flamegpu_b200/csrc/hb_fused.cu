@@ -27,7 +27,10 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <cuda.h>
+
 #include <mutex>
+#include <vector>
 
 #include "hb_common.cuh"
 #include "hb_physics.cuh"
@@ -151,15 +154,25 @@ __device__ __noinline__ void boundary_face(const Smem<T, TY, TX> &s, int kc, T n
   if (!ghost(type, false, C, n0, n1, hb, wlb, qxb, qyb, G)) return;
   if (C.h < hs && G.h < hs) return;
   Cell<T> eL = C, eR = G;
-  const T ux_l = eL.h < hs ? T(0) : eL.qx / eL.h;
-  const T uy_l = eL.h < hs ? T(0) : eL.qy / eL.h;
-  const T ux_r = eR.h < hs ? T(0) : eR.qx / eR.h;
-  const T uy_r = eR.h < hs ? T(0) : eR.qy / eR.h;
+  // the same arithmetic as interior faces, so that a state symmetric about a
+  // wall gives bitwise the same pressure flux on both sides of a cell
+  T ux_l, uy_l, ux_r, uy_r;
+  if constexpr (FAST) {
+    const T il = eL.h < hs ? T(0) : T(1) / eL.h;
+    const T ir = eR.h < hs ? T(0) : T(1) / eR.h;
+    ux_l = eL.qx * il; uy_l = eL.qy * il;
+    ux_r = eR.qx * ir; uy_r = eR.qy * ir;
+  } else {
+    ux_l = eL.h < hs ? T(0) : eL.qx / eL.h;
+    uy_l = eL.h < hs ? T(0) : eL.qy / eL.h;
+    ux_r = eR.h < hs ? T(0) : eR.qx / eR.h;
+    uy_r = eR.h < hs ? T(0) : eR.qy / eR.h;
+  }
   hydro2(C.wl, G.wl, eL, eR);
   const T u_L = ux_l * n0 + uy_l * n1, u_R = ux_r * n0 + uy_r * n1;
   const T v_L = -ux_l * n1 + uy_l * n0, v_R = -ux_r * n1 + uy_r * n0;
   T Fh, Fn, Ft;
-  if (hllc<T, false>(eL.h, eR.h, u_L, u_R, v_L, v_R, Fh, Fn, Ft)) {
+  if (hllc<T, FAST>(eL.h, eR.h, u_L, u_R, v_L, v_R, Fh, Fn, Ft)) {
     fh = Fh;
     fx = Fn * n0 + Ft * (-n1);
     fy = Fn * n1 + Ft * n0;
@@ -254,9 +267,93 @@ __device__ void bc_values_exact(const hb_instance &in, double t, BcTable *out) {
   }
 }
 
-// Workspace layout: [n_tiles] TilePartial, then [n_instances] BcTable.
+
+// Last tile of an instance in a step: reduce the tiles' partials and advance
+// the control block (HP/SWE_CUDA.py:818-831): dt = min over cells of
+// CFL * dx / speed (60 s for dry cells), the 10x growth cap, the clip to the
+// next export time, t += dt, FP64 volume / outflow / rain totals, and the rain
+// rate and boundary values of the next step.  Called by every thread of the
+// CTA that finished the instance's last tile.
+template <typename T, int NT>
+__device__ void finalize_instance(const hb_instance &in, int ii, TilePartial *partials,
+                                  BcTable *bct, double (*red_d)[NT / 32], double *red_s,
+                                  int *red_i) {
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  hb_ctrl *ctrl = in.ctrl;
+  __threadfence();
+  const int nt = in.tiles_x * in.tiles_y;
+  double v = 0, o = 0, sm = 0;
+  int dry = 0;
+  for (int k = tid; k < nt; k += NT) {
+    const TilePartial *pp = partials + in.tile_begin + k;
+    v += __ldcg(&pp->volume);
+    o += __ldcg(&pp->outflow);
+    sm = fmax(sm, __ldcg(&pp->smax));
+    dry |= __ldcg(&pp->any_dry);
+  }
+  v = warp_sum(v);
+  o = warp_sum(o);
+  sm = warp_max(sm);
+  dry = __any_sync(0xffffffffu, dry);
+  if (lane == 0) {
+    red_d[0][wid] = v;
+    red_d[1][wid] = o;
+    red_s[wid] = sm;
+    red_i[wid] = dry;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double V = 0, O = 0, SM = 0;
+    int D = 0;
+    for (int w = 0; w < NT / 32; w++) {
+      V += red_d[0][w];
+      O += red_d[1][w];
+      SM = fmax(SM, red_s[w]);
+      D |= red_i[w];
+    }
+    const double dtn = ctrl->dt, tn = ctrl->t, dxd = in.dx;
+    // min over cells of CFL*dx/speed; the division is monotone, so dividing
+    // once by the largest speed gives the same value.
+    double cand = INFINITY;
+    if (SM > 0.0) cand = (double)((T)in.cfl * (T)in.dx / (T)SM);
+    if (D) cand = fmin(cand, 60.0);
+    double dtnew = (cand == INFINITY) ? dtn : cand;
+    const double upper = dtn * 10.0;
+    if (upper < dtnew) dtnew = upper;  // Python min(self.dt, time_upper)
+    const double next_export = (double)(ctrl->export_n + 1) * ctrl->export_step;
+    if (ctrl->export_step > 0.0 && dtnew + tn >= next_export) {
+      dtnew = next_export - tn;
+      ctrl->export_n += 1;
+      ctrl->exports += 1;
+      if (ctrl->halt_on_export) ctrl->halted = 1;
+    }
+    if (in.dt_replay && ctrl->step < in.n_replay) dtnew = in.dt_replay[ctrl->step];
+    if (!isfinite(dtnew)) ctrl->status |= 1;
+    ctrl->volume = V * dxd * dxd;
+    ctrl->outflow_volume += O * dtn * dxd;
+    ctrl->rain_volume += ctrl->rain_rate * dtn * dxd * dxd * (double)in.n_valid;
+    const double tnew = tn + dtnew;
+    ctrl->dt = dtnew;
+    ctrl->t = tnew;
+    ctrl->cur = 1 - ctrl->cur;
+    ctrl->step += 1;
+    if (tnew >= ctrl->t_end) ctrl->halted = 1;
+    ctrl->rain_rate = rain_rate_at(in, ctrl, tnew);
+    bc_values_exact(in, tnew, &bct[ii]);
+    bc_values_at(in, ctrl, tnew);
+    __threadfence();
+    ctrl->tiles_done = 0u;
+  }
+}
+
+// Workspace layout: [n_tiles] TilePartial, [n_instances] BcTable, then
+// [n_instances][kMapsPerInstance] CUtensorMap (128-byte aligned).
 inline size_t ws_partials_bytes(int n_tiles) {
   return ((size_t)n_tiles * sizeof(TilePartial) + 255) & ~(size_t)255;
+}
+inline size_t ws_maps_offset(const hb_fused_batch *b) {
+  return (ws_partials_bytes(b->n_tiles) + (size_t)b->n_instances * sizeof(BcTable) + 255) &
+         ~(size_t)255;
 }
 
 // ---------------------------------------------------------------------------
@@ -269,7 +366,7 @@ fused_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restri
   using S = Smem<T, TY, TX>;
   constexpr int SW = S::SW, SH = S::SH;
   constexpr int V = 16 / sizeof(T);  // elements per 16-byte vector
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   S &s = *reinterpret_cast<S *>(smem_raw);
   const int tid = threadIdx.x;
   const T hs = T(kHSmall), g = T(kG);
@@ -581,73 +678,602 @@ fused_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restri
     }
     __syncthreads();
 
-    if (s.last) {
-      // --- finalize this instance: reduce its tiles' partials
-      __threadfence();
-      const int nt = in.tiles_x * in.tiles_y;
-      double v = 0, o = 0, sm = 0;
-      int dry = 0;
-      for (int k = tid; k < nt; k += kNT) {
-        const TilePartial *pp = partials + in.tile_begin + k;
-        v += __ldcg(&pp->volume);
-        o += __ldcg(&pp->outflow);
-        sm = fmax(sm, __ldcg(&pp->smax));
-        dry |= __ldcg(&pp->any_dry);
-      }
-      v = warp_sum(v);
-      o = warp_sum(o);
-      sm = warp_max(sm);
-      dry = __any_sync(0xffffffffu, dry);
-      if (lane == 0) {
-        s.red_d[0][wid] = v;
-        s.red_d[1][wid] = o;
-        s.red_s[wid] = sm;
-        s.red_i[wid] = dry;
-      }
-      __syncthreads();
-      if (tid == 0) {
-        double V = 0, O = 0, SM = 0;
-        int D = 0;
-        for (int w = 0; w < kNT / 32; w++) {
-          V += s.red_d[0][w];
-          O += s.red_d[1][w];
-          SM = fmax(SM, s.red_s[w]);
-          D |= s.red_i[w];
-        }
-        const double dtn = ctrl->dt, tn = ctrl->t, dxd = in.dx;
-        // dt = min over cells of CFL*dx/speed (60 for dry cells); the
-        // division is monotone, so dividing once by the max speed is exact.
-        double cand = INFINITY;
-        if (SM > 0.0) cand = (double)((T)in.cfl * (T)in.dx / (T)SM);
-        if (D) cand = fmin(cand, 60.0);
-        double dtnew = (cand == INFINITY) ? dtn : cand;
-        const double upper = dtn * 10.0;
-        if (upper < dtnew) dtnew = upper;  // Python min(self.dt, time_upper)
-        const double next_export = (double)(ctrl->export_n + 1) * ctrl->export_step;
-        if (ctrl->export_step > 0.0 && dtnew + tn >= next_export) {
-          dtnew = next_export - tn;
-          ctrl->export_n += 1;
-          ctrl->exports += 1;
-          if (ctrl->halt_on_export) ctrl->halted = 1;
-        }
-        if (in.dt_replay && ctrl->step < in.n_replay) dtnew = in.dt_replay[ctrl->step];
-        if (!isfinite(dtnew)) ctrl->status = 1;
-        ctrl->volume = V * dxd * dxd;
-        ctrl->outflow_volume += O * dtn * dxd;
-        ctrl->rain_volume += ctrl->rain_rate * dtn * dxd * dxd * (double)in.n_valid;
-        const double tnew = tn + dtnew;
-        ctrl->dt = dtnew;
-        ctrl->t = tnew;
-        ctrl->cur = 1 - ctrl->cur;
-        ctrl->step += 1;
-        if (tnew >= ctrl->t_end) ctrl->halted = 1;
-        ctrl->rain_rate = rain_rate_at(in, ctrl, tnew);
-        bc_values_exact(in, tnew, &bct[ii]);
-        bc_values_at(in, ctrl, tnew);
-        __threadfence();
-        ctrl->tiles_done = 0u;
+    if (s.last) finalize_instance<T, kNT>(in, ii, partials, bct, s.red_d, s.red_s, s.red_i);
+    __syncthreads();
+  }
+}
+
+
+// ===========================================================================
+// Row-walking kernel over TMA-staged tiles.
+//
+// A CTA of 4 warps owns a tile of 32 columns x TY rows.  One elected thread
+// stages h, qx, qy, z (tile + 2-cell halo, 4 columns each side), the tile's
+// h_max and the cell codes into shared memory with 2-D TMA loads completing
+// on an mbarrier.  Each warp then walks TY/4 consecutive rows, lane j owning
+// column j:
+//  * per-cell MUSCL slopes are formed once (x from the row's neighbours, y
+//    from a sliding window of the column's rows held in registers) and shared
+//    by the cell's two faces along that axis;
+//  * the face to the south is evaluated in registers and reused as the next
+//    row's north face; the face to the west is evaluated by each lane and
+//    handed to the west neighbour as its east face by a warp shuffle;
+//  * the cell update (gather, rain, friction, h_max, CFL speed, volume) runs
+//    on the same registers and writes the new state with coalesced stores.
+// Every face is still evaluated once.
+// ===========================================================================
+constexpr int kRowsNW = 4;             // warps per CTA
+constexpr int kRowsNT = 32 * kRowsNW;  // threads per CTA
+constexpr int kTW = 32;                // tile width (one warp)
+constexpr int kSWF = kTW + 8;          // staged field row: cols -4..35
+constexpr int kSWC = kTW + 32;         // staged code row: cols -16..47
+constexpr int kMapsPerInstance = 9;    // h0 h1 qx0 qx1 qy0 qy1 z h_max code
+
+template <typename T, int TY>
+struct RowsSmem {
+  static constexpr int SH = TY + 4;
+  static constexpr int R = TY / kRowsNW;
+  T f[4][SH * kSWF];          // h, qx, qy, z
+  T hmax[TY * kTW];           // h_max of the tile's cells
+  uint8_t code[SH * kSWC];
+  alignas(8) unsigned long long bar;
+  T xe[kRowsNW][R][4];        // face between cols 31 | 32: fh, fx, fy, sa
+  T sxw[kRowsNW][R][4];       // x-slope of col -1: h, z, qx, qy
+  double bc[HB_MAX_CLASSES][4];
+  int bctype[HB_MAX_CLASSES];
+  T ddatum[9];
+  double red_d[2][kRowsNW];
+  double red_s[kRowsNW];
+  int red_i[kRowsNW];
+  int last;
+  static constexpr unsigned kTxBytes =
+      (unsigned)(4 * SH * kSWF * sizeof(T) + TY * kTW * sizeof(T) + SH * kSWC);
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned phase) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: false if the phase did not complete within `budget` cycles.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned phase,
+                                          long long budget) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, phase)) {
+    if (clock64() - t0 > budget) return false;
+  }
+  return true;
+}
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y,
+                                            unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+template <typename T>
+struct Slope {
+  T h, z, qx, qy;
+};
+
+// minmod slope of cell c between its minus-side neighbour m and plus-side
+// neighbour p; a no-data neighbour is replaced by c itself, as the reference
+// does with a missing neighbour id (HC/flucCal_2ndOrder_jh_improved_Kernel.cu:416-428).
+template <typename T>
+__device__ __forceinline__ Slope<T> slope_of(const Cell<T> &c, const Cell<T> &m, bool vm,
+                                             const Cell<T> &p, bool vp) {
+  const Cell<T> &mm = vm ? m : c;
+  const Cell<T> &pp = vp ? p : c;
+  Slope<T> s;
+  s.h = minmod(c.h - mm.h, pp.h - c.h);
+  s.z = minmod(c.z - mm.z, pp.z - c.z);
+  s.qx = minmod(c.qx - mm.qx, pp.qx - c.qx);
+  s.qy = minmod(c.qy - mm.qy, pp.qy - c.qy);
+  return s;
+}
+
+// Edge state of c on its plus side (sign = +1) or minus side (sign = -1).
+template <typename T>
+__device__ __forceinline__ Cell<T> edge_of(const Cell<T> &c, const Slope<T> &s, T sign) {
+  Cell<T> e;
+  e.h = c.h + T(0.5) * (sign * s.h);
+  e.z = c.z + T(0.5) * (sign * s.z);
+  e.wl = c.wl;
+  if (c.h < T(kHSmall)) {
+    e.qx = T(0);
+    e.qy = T(0);
+  } else {
+    e.qx = c.qx + T(0.5) * (sign * s.qx);
+    e.qy = c.qy + T(0.5) * (sign * s.qy);
+  }
+  return e;
+}
+
+// Face between valid cells A (west/south) and B (east/north) from A's side,
+// given both MUSCL edge states.  DIR 0: normal +x; DIR 1: normal +y.
+template <typename T, bool FAST, int DIR>
+__device__ __forceinline__ FaceOut<T> face_edges(const Cell<T> &A, const Cell<T> &B,
+                                                 Cell<T> eL, Cell<T> eR) {
+  const T hs = T(kHSmall), g = T(kG);
+  FaceOut<T> o{T(0), T(0), T(0), T(0), T(0)};
+  if (A.h < hs && B.h < hs) return o;
+  T ux_l, uy_l, ux_r, uy_r;
+  if constexpr (FAST) {
+    const T il = eL.h < hs ? T(0) : T(1) / eL.h;
+    const T ir = eR.h < hs ? T(0) : T(1) / eR.h;
+    ux_l = eL.qx * il; uy_l = eL.qy * il;
+    ux_r = eR.qx * ir; uy_r = eR.qy * ir;
+  } else {
+    ux_l = eL.h < hs ? T(0) : eL.qx / eL.h;
+    uy_l = eL.h < hs ? T(0) : eL.qy / eL.h;
+    ux_r = eR.h < hs ? T(0) : eR.qx / eR.h;
+    uy_r = eR.h < hs ? T(0) : eR.qy / eR.h;
+  }
+  hydro2(A.wl, B.wl, eL, eR);
+  T Fh, Fn, Ft;
+  if (DIR == 0) {
+    if (hllc<T, FAST>(eL.h, eR.h, ux_l, ux_r, uy_l, uy_r, Fh, Fn, Ft)) {
+      o.fh = Fh; o.fx = Fn; o.fy = Ft;
+    }
+  } else {
+    if (hllc<T, FAST>(eL.h, eR.h, uy_l, uy_r, -ux_l, -ux_r, Fh, Fn, Ft)) {
+      o.fh = Fh; o.fx = -Ft; o.fy = Fn;
+    }
+  }
+  o.sa = T(0.5) * g * (A.h + eL.h) * (eL.z - A.z);
+  o.sb = T(0.5) * g * (B.h + eR.h) * (eR.z - B.z);
+  return o;
+}
+
+// Boundary face of valid cell C with outward normal (n0, n1): ghost from
+// C's class.  Flux from C's side and C's bed-slope term.
+template <typename T, bool FAST>
+__device__ __noinline__ void ghost_face(const Cell<T> C, int cls, int type, const double *bcv,
+                                        T n0, T n1, T datum, T *out) {
+  const T hs = T(kHSmall), g = T(kG);
+  out[0] = out[1] = out[2] = out[3] = T(0);
+  Cell<T> G;
+  const T hb = (T)bcv[0], wlb = (T)(bcv[1] - (double)datum);
+  const T qxb = (T)bcv[2], qyb = (T)bcv[3];
+  if (!ghost(type, false, C, n0, n1, hb, wlb, qxb, qyb, G)) return;
+  (void)cls;
+  if (C.h < hs && G.h < hs) return;
+  Cell<T> eL = C, eR = G;
+  T ux_l, uy_l, ux_r, uy_r;
+  if constexpr (FAST) {
+    const T il = eL.h < hs ? T(0) : T(1) / eL.h;
+    const T ir = eR.h < hs ? T(0) : T(1) / eR.h;
+    ux_l = eL.qx * il; uy_l = eL.qy * il;
+    ux_r = eR.qx * ir; uy_r = eR.qy * ir;
+  } else {
+    ux_l = eL.h < hs ? T(0) : eL.qx / eL.h;
+    uy_l = eL.h < hs ? T(0) : eL.qy / eL.h;
+    ux_r = eR.h < hs ? T(0) : eR.qx / eR.h;
+    uy_r = eR.h < hs ? T(0) : eR.qy / eR.h;
+  }
+  hydro2(C.wl, G.wl, eL, eR);
+  const T u_L = ux_l * n0 + uy_l * n1, u_R = ux_r * n0 + uy_r * n1;
+  const T v_L = -ux_l * n1 + uy_l * n0, v_R = -ux_r * n1 + uy_r * n0;
+  T Fh, Fn, Ft;
+  if (hllc<T, FAST>(eL.h, eR.h, u_L, u_R, v_L, v_R, Fh, Fn, Ft)) {
+    out[0] = Fh;
+    out[1] = Fn * n0 + Ft * (-n1);
+    out[2] = Fn * n1 + Ft * n0;
+  }
+  out[3] = T(0.5) * g * (C.h + eL.h) * (eL.z - C.z);
+}
+
+template <typename T, int TY>
+struct RowsView {
+  const RowsSmem<T, TY> &s;
+  __device__ __forceinline__ int fi(int i, int j) const { return (i + 2) * kSWF + (j + 4); }
+  __device__ __forceinline__ Cell<T> cell(int i, int j) const {
+    const int k = fi(i, j);
+    Cell<T> c;
+    c.h = s.f[0][k];
+    c.qx = s.f[1][k];
+    c.qy = s.f[2][k];
+    c.z = s.f[3][k];
+    c.wl = c.z + c.h;  // the reference stores wl = z + h after every update
+    return c;
+  }
+  __device__ __forceinline__ uint8_t code(int i, int j) const {
+    return s.code[(i + 2) * kSWC + (j + 16)];
+  }
+};
+
+// Face between A (minus side) and B (plus side) along DIR, any validity.
+// eA / eB: MUSCL edges (used only when both are valid).
+template <typename T, bool FAST, int DIR, int TY>
+__device__ __forceinline__ FaceOut<T> face_any(const RowsSmem<T, TY> &s, const Cell<T> &A,
+                                               uint8_t ca, const Cell<T> &B, uint8_t cb,
+                                               const Cell<T> &eA, const Cell<T> &eB, T datum) {
+  const bool va = is_valid(ca), vb = is_valid(cb);
+  if (va && vb) return face_edges<T, FAST, DIR>(A, B, eA, eB);
+  FaceOut<T> o{T(0), T(0), T(0), T(0), T(0)};
+  const T n0 = DIR == 0 ? T(1) : T(0), n1 = DIR == 0 ? T(0) : T(1);
+  T out[4];
+  if (va) {
+    const int cls = ca >> 4;
+    ghost_face<T, FAST>(A, cls, s.bctype[cls], s.bc[cls], n0, n1, datum, out);
+    o.fh = out[0]; o.fx = out[1]; o.fy = out[2]; o.sa = out[3];
+  } else if (vb) {
+    const int cls = cb >> 4;
+    ghost_face<T, FAST>(B, cls, s.bctype[cls], s.bc[cls], -n0, -n1, datum, out);
+    o.fh = -out[0]; o.fx = -out[1]; o.fy = -out[2]; o.sb = out[3];
+  }
+  return o;
+}
+
+template <typename T, int TY, bool FAST>
+__global__ void __launch_bounds__(kRowsNT)
+rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restrict__ tile_inst,
+                 int n_tiles, TilePartial *__restrict__ partials, BcTable *__restrict__ bct,
+                 const CUtensorMap *__restrict__ maps) {
+  using S = RowsSmem<T, TY>;
+  constexpr int R = S::R;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  S &s = *reinterpret_cast<S *>(smem_raw);
+  const RowsView<T, TY> V{s};
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const T hs = T(kHSmall), g = T(kG);
+  if (tid == 0) {
+    mbar_init(&s.bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  unsigned phase = 0;
+
+  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int ii = tile_inst[tile];
+    const hb_instance &in = insts[ii];
+    hb_ctrl *ctrl = in.ctrl;
+    if (ctrl->halted) continue;
+    const int lt = tile - in.tile_begin;
+    const int tyi = lt / in.tiles_x, txi = lt - tyi * in.tiles_x;
+    const int y0 = tyi * TY, x0 = txi * kTW;
+    const int cur = ctrl->cur;
+    const double t = ctrl->t;
+    const T dt = (T)ctrl->dt;
+    const T dx = (T)in.dx;
+    const T rain = (T)ctrl->rain_rate;
+    const bool first = (t == 0.0);
+    const int P = in.pitch;
+    const CUtensorMap *m = maps + (size_t)ii * kMapsPerInstance;
+
+    if (tid == 0) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_expect_tx(&s.bar, S::kTxBytes);
+      tma_load_2d(s.f[0], m + 0 + cur, x0, y0, &s.bar);
+      tma_load_2d(s.f[1], m + 2 + cur, x0, y0, &s.bar);
+      tma_load_2d(s.f[2], m + 4 + cur, x0, y0, &s.bar);
+      tma_load_2d(s.f[3], m + 6, x0, y0, &s.bar);
+      tma_load_2d(s.hmax, m + 7, x0 + HB_PAD_X, y0 + HB_PAD_Y, &s.bar);
+      tma_load_2d(s.code, m + 8, x0, y0, &s.bar);
+    }
+    if (tid < HB_MAX_CLASSES) {
+      s.bctype[tid] = in.bc_type[tid];
+      for (int q = 0; q < 4; q++) s.bc[tid][q] = bct[ii].v[tid][q];
+    }
+    T datum_tile = T(0);
+    if (in.datum) {
+      const int by = y0 / HB_DATUM_BLOCK, bx = x0 / HB_DATUM_BLOCK;
+      datum_tile = (T)in.datum[by * in.datum_nx + bx];
+      if (tid >= 32 && tid < 41) {
+        const int k = tid - 32, dyb = k / 3 - 1, dxb = k % 3 - 1;
+        const int yy = min(max(by + dyb, 0), in.datum_ny - 1);
+        const int xx = min(max(bx + dxb, 0), in.datum_nx - 1);
+        s.ddatum[k] = (T)in.datum[yy * in.datum_nx + xx] - datum_tile;
       }
     }
+    const bool arrived = mbar_wait(&s.bar, phase, 4000000000LL);
+    if (__syncthreads_or(!arrived)) {
+      // the tile's data did not arrive within the budget: flag it, wait once
+      // more (bounded) for the copy in flight, and leave without touching the
+      // state; the host sees ctrl->status
+      if (tid == 0) atomicOr(&ctrl->status, 2);
+      mbar_wait(&s.bar, phase, 4000000000LL);
+      return;
+    }
+    phase ^= 1u;
+    if (in.datum) {
+      __syncthreads();  // ddatum visible
+      const int by0 = (y0 / HB_DATUM_BLOCK) * HB_DATUM_BLOCK;
+      const int bx0 = (x0 / HB_DATUM_BLOCK) * HB_DATUM_BLOCK;
+      // halo rows (2 above, 2 below) and halo columns (4 each side)
+      constexpr int NH = 4 * kSWF + TY * 8;
+      for (int k = tid; k < NH; k += kRowsNT) {
+        int i, j;
+        if (k < 4 * kSWF) {
+          const int r = k / kSWF;
+          i = r < 2 ? r - 2 : TY + (r - 2);
+          j = k % kSWF - 4;
+        } else {
+          const int q = k - 4 * kSWF;
+          i = q / 8;
+          const int c = q % 8;
+          j = c < 4 ? c - 4 : kTW + (c - 4);
+        }
+        const int ry = y0 + i, rx = x0 + j;
+        const int dyb = ry < by0 ? 0 : (ry >= by0 + HB_DATUM_BLOCK ? 2 : 1);
+        const int dxb = rx < bx0 ? 0 : (rx >= bx0 + HB_DATUM_BLOCK ? 2 : 1);
+        if (dyb != 1 || dxb != 1) s.f[3][V.fi(i, j)] += s.ddatum[dyb * 3 + dxb];
+      }
+    }
+    __syncthreads();
+
+    const int r0 = w * R;
+    // --- per warp: x-slope of column -1 and the face between columns 31|32
+    if (lane < R) {
+      const int i = r0 + lane;
+      const Cell<T> cm2 = V.cell(i, -2), cm1 = V.cell(i, -1), c0 = V.cell(i, 0);
+      const Slope<T> sm1 = slope_of(cm1, cm2, is_valid(V.code(i, -2)), c0,
+                                    is_valid(V.code(i, 0)));
+      s.sxw[w][lane][0] = sm1.h;
+      s.sxw[w][lane][1] = sm1.z;
+      s.sxw[w][lane][2] = sm1.qx;
+      s.sxw[w][lane][3] = sm1.qy;
+      const Cell<T> a = V.cell(i, 31), b = V.cell(i, 32);
+      const uint8_t ca = V.code(i, 31), cb = V.code(i, 32);
+      const Slope<T> sa = slope_of(a, V.cell(i, 30), is_valid(V.code(i, 30)), b, is_valid(cb));
+      const Slope<T> sb = slope_of(b, a, is_valid(ca), V.cell(i, 33), is_valid(V.code(i, 33)));
+      const FaceOut<T> f = face_any<T, FAST, 0>(s, a, ca, b, cb, edge_of(a, sa, T(1)),
+                                                edge_of(b, sb, T(-1)), datum_tile);
+      s.xe[w][lane][0] = f.fh;
+      s.xe[w][lane][1] = f.fx;
+      s.xe[w][lane][2] = f.fy;
+      s.xe[w][lane][3] = f.sa;
+    }
+    __syncwarp();
+
+    // --- column window: rows r0-2 .. r0+2
+    const int j = lane;
+    Cell<T> cN = V.cell(r0 - 1, j), cC = V.cell(r0, j), cS = V.cell(r0 + 1, j);
+    uint8_t kN = V.code(r0 - 1, j), kC = V.code(r0, j), kS = V.code(r0 + 1, j);
+    Slope<T> syC, syS;
+    FaceOut<T> nf;
+    {
+      const Cell<T> cNN = V.cell(r0 - 2, j);
+      const uint8_t kNN = V.code(r0 - 2, j);
+      const Cell<T> cSS = V.cell(r0 + 2, j);
+      const uint8_t kSS = V.code(r0 + 2, j);
+      // y-slopes: minus side = south (row + 1), plus side = north (row - 1)
+      const Slope<T> syN = slope_of(cN, cC, is_valid(kC), cNN, is_valid(kNN));
+      syC = slope_of(cC, cS, is_valid(kS), cN, is_valid(kN));
+      syS = slope_of(cS, cSS, is_valid(kSS), cC, is_valid(kC));
+      // face between rows r0-1 (north) and r0 (south), from the south side
+      nf = face_any<T, FAST, 1>(s, cC, kC, cN, kN, edge_of(cC, syC, T(1)),
+                                edge_of(cN, syN, T(-1)), datum_tile);
+    }
+    double vol = 0.0, outf = 0.0, smax = 0.0;
+    int any_dry = 0;
+    T *hout = (T *)in.h[1 - cur];
+    T *qxout = (T *)in.qx[1 - cur];
+    T *qyout = (T *)in.qy[1 - cur];
+    T *hmaxg = (T *)in.h_max;
+    const int rx = x0 + j;
+
+#pragma unroll 1
+    for (int i = r0; i < r0 + R; ++i) {
+      const Cell<T> cW = V.cell(i, j - 1), cE = V.cell(i, j + 1);
+      const uint8_t kW = V.code(i, j - 1), kE = V.code(i, j + 1);
+      const bool vW = is_valid(kW), vE = is_valid(kE), vC = is_valid(kC);
+      const Slope<T> sxC = slope_of(cC, cW, vW, cE, vE);
+      Slope<T> sxW;
+      sxW.h = __shfl_up_sync(0xffffffffu, sxC.h, 1);
+      sxW.z = __shfl_up_sync(0xffffffffu, sxC.z, 1);
+      sxW.qx = __shfl_up_sync(0xffffffffu, sxC.qx, 1);
+      sxW.qy = __shfl_up_sync(0xffffffffu, sxC.qy, 1);
+      if (lane == 0) {
+        sxW.h = s.sxw[w][i - r0][0];
+        sxW.z = s.sxw[w][i - r0][1];
+        sxW.qx = s.sxw[w][i - r0][2];
+        sxW.qy = s.sxw[w][i - r0][3];
+      }
+      // west face (this cell is B) -> the west neighbour's east face
+      const FaceOut<T> wf = face_any<T, FAST, 0>(s, cW, kW, cC, kC, edge_of(cW, sxW, T(1)),
+                                                 edge_of(cC, sxC, T(-1)), datum_tile);
+      T ef_h = __shfl_down_sync(0xffffffffu, wf.fh, 1);
+      T ef_x = __shfl_down_sync(0xffffffffu, wf.fx, 1);
+      T ef_y = __shfl_down_sync(0xffffffffu, wf.fy, 1);
+      T ef_a = __shfl_down_sync(0xffffffffu, wf.sa, 1);
+      if (lane == 31) {
+        ef_h = s.xe[w][i - r0][0];
+        ef_x = s.xe[w][i - r0][1];
+        ef_y = s.xe[w][i - r0][2];
+        ef_a = s.xe[w][i - r0][3];
+      }
+      // south face (this cell is B, the row below is A)
+      const FaceOut<T> sf = face_any<T, FAST, 1>(s, cS, kS, cC, kC, edge_of(cS, syS, T(1)),
+                                                 edge_of(cC, syC, T(-1)), datum_tile);
+      const int ry = y0 + i;
+      if (vC) {
+        const T hc = cC.h;
+        bool active = first || hc > hs;
+        if (!active) {
+          const bool bugE = (ry == in.bug_y && rx + 1 == in.bug_x);
+          const bool bugW = (ry == in.bug_y && rx - 1 == in.bug_x);
+          const bool bugN = (ry - 1 == in.bug_y && rx == in.bug_x);
+          const bool bugS = (ry + 1 == in.bug_y && rx == in.bug_x);
+          active = (vE && !bugE && cE.h > hs) || (is_valid(kN) && !bugN && cN.h > hs) ||
+                   (vW && !bugW && cW.h > hs) || (is_valid(kS) && !bugS && cS.h > hs);
+        }
+        T hu = T(0), qxu = T(0), qyu = T(0);
+        if (active) {
+          if constexpr (FAST) {
+            const T r = dt / dx;
+            hu = ((wf.fh + sf.fh) - (ef_h + nf.fh)) * r;
+            qxu = ((wf.fx + sf.fx) - (ef_x + nf.fx) - ef_a + wf.sb) * r;
+            qyu = ((wf.fy + sf.fy) - (ef_y + nf.fy) - nf.sa + sf.sb) * r;
+          } else {
+            hu -= (ef_h / dx) * dt;
+            qxu -= (ef_x / dx) * dt;
+            qyu -= (ef_y / dx) * dt;
+            qxu -= (ef_a / dx) * dt;
+            hu -= (nf.fh / dx) * dt;
+            qxu -= (nf.fx / dx) * dt;
+            qyu -= (nf.fy / dx) * dt;
+            qyu -= (nf.sa / dx) * dt;
+            hu -= (-wf.fh / dx) * dt;
+            qxu -= (-wf.fx / dx) * dt;
+            qyu -= (-wf.fy / dx) * dt;
+            qxu -= (-wf.sb / dx) * dt;
+            hu -= (-sf.fh / dx) * dt;
+            qxu -= (-sf.fx / dx) * dt;
+            qyu -= (-sf.fy / dx) * dt;
+            qyu -= (-sf.sb / dx) * dt;
+          }
+          const bool bE = !vE, bW = !vW, bN = !is_valid(kN), bS = !is_valid(kS);
+          if (bE | bW | bN | bS) {
+            double o = 0.0;
+            if (bE) o += (double)ef_h;
+            if (bN) o += (double)nf.fh;
+            if (bW) o -= (double)wf.fh;
+            if (bS) o -= (double)sf.fh;
+            outf += o;
+          }
+        }
+        hu += rain * dt;
+        T h = hc + hu;
+        T qx = cC.qx, qy = cC.qy;
+        T sgh = T(0);
+        if (h < hs) {
+          qx = T(0);
+          qy = T(0);
+        } else {
+          const T n = (T)in.manning[kC & 15];
+          qx += qxu;
+          qy += qyu;
+          sgh = FAST ? (T)sqrtf((float)(g * h)) : (T)__fsqrt_rn((float)(g * h));
+          if constexpr (FAST) {
+            if (n > T(0)) {
+              const T ih = T(1) / h;
+              const T q_norm = sqrtf(qx * qx + qy * qy);
+              const T a = dt * g * n * n * exp2f(-__log2f(h) * (T(1) / T(3))) * ih * ih;
+              const T fct = T(2) / (T(1) + sqrtf(T(1) + T(4) * a * q_norm));
+              const T lim = T(5) * h * sgh;
+              if (fabsf(qx) > T(1.0e-10)) {
+                const T temp = qx * fct;
+                if (fabsf(temp) > lim) {
+                  qx = T(2) * temp - qx;
+                  if (qx * temp <= T(0)) qx = T(0);
+                } else {
+                  qx = temp;
+                }
+              }
+              if (fabsf(qy) > T(1.0e-10)) {
+                const T temp = qy * fct;
+                if (fabsf(temp) > lim) {
+                  qy = T(2) * temp - qy;
+                  if (qy * temp <= T(0)) qy = T(0);
+                } else {
+                  qy = temp;
+                }
+              }
+            }
+          } else {
+            const T C_f = g * n * n * pow(h, T(-1.0 / 3.0));
+            const T q_norm = sqrt(qx * qx + qy * qy);
+            if (n > T(0)) {
+              if (fabs(qx) > T(1.0e-10)) {
+                T temp = (T(1) - sqrt(T(1) + (T(4) * dt * C_f) / (h * h) * q_norm)) /
+                         (T(-2) * dt * C_f / (h * h) * (q_norm / qx));
+                if (fabs(temp) > T(5) * h * sqrt(h * g)) {
+                  qx = T(2) * temp - qx;
+                  if (qx * temp <= T(0)) qx = T(0);
+                } else {
+                  qx = temp;
+                }
+              }
+              if (fabs(qy) > T(1.0e-10)) {
+                T temp = (T(1) - sqrt(T(1) + (T(4) * dt * C_f) / (h * h) * q_norm)) /
+                         (T(-2) * dt * C_f / (h * h) * (q_norm / qy));
+                if (fabs(temp) > T(5) * h * sqrt(h * g)) {
+                  qy = T(2) * temp - qy;
+                  if (qy * temp <= T(0)) qy = T(0);
+                } else {
+                  qy = temp;
+                }
+              }
+            }
+          }
+        }
+        const size_t go = (size_t)(ry + HB_PAD_Y) * P + (rx + HB_PAD_X);
+        hout[go] = h;
+        qxout[go] = qx;
+        qyout[go] = qy;
+        hmaxg[go] = fmax(h, s.hmax[i * kTW + j]);
+        if (h > hs) {
+          smax = fmax(smax, (double)(sgh + fmax(fabs(qx), fabs(qy)) / h));
+        } else {
+          any_dry = 1;
+        }
+        vol += (double)h;
+      }
+      // slide the column window down one row
+      nf = sf;
+      cN = cC; kN = kC;
+      cC = cS; kC = kS;
+      syC = syS;
+      if (i + 1 < r0 + R) {
+        cS = V.cell(i + 2, j);
+        kS = V.code(i + 2, j);
+        const Cell<T> cSS = V.cell(i + 3, j);
+        const uint8_t kSS = V.code(i + 3, j);
+        syS = slope_of(cS, cSS, is_valid(kSS), cC, is_valid(kC));
+      }
+    }
+
+    // --- tile partials and the instance's last-tile finalize
+    vol = warp_sum(vol);
+    outf = warp_sum(outf);
+    smax = warp_max(smax);
+    any_dry = __any_sync(0xffffffffu, any_dry);
+    if (lane == 0) {
+      s.red_d[0][w] = vol;
+      s.red_d[1][w] = outf;
+      s.red_s[w] = smax;
+      s.red_i[w] = any_dry;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      TilePartial p;
+      p.volume = p.outflow = p.smax = 0.0;
+      p.any_dry = 0;
+      p.pad = 0;
+      for (int q = 0; q < kRowsNW; q++) {
+        p.volume += s.red_d[0][q];
+        p.outflow += s.red_d[1][q];
+        p.smax = fmax(p.smax, s.red_s[q]);
+        p.any_dry |= s.red_i[q];
+      }
+      partials[tile] = p;
+      __threadfence();
+      const unsigned n_inst_tiles = (unsigned)(in.tiles_x * in.tiles_y);
+      s.last = (atomicAdd(&ctrl->tiles_done, 1u) == n_inst_tiles - 1);
+    }
+    __syncthreads();
+    if (s.last) finalize_instance<T, kRowsNT>(in, ii, partials, bct, s.red_d, s.red_s, s.red_i);
     __syncthreads();
   }
 }
@@ -706,10 +1332,113 @@ int launch_steps(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   TilePartial *parts = reinterpret_cast<TilePartial *>(b->workspace);
   BcTable *bct = reinterpret_cast<BcTable *>((char *)b->workspace + ws_partials_bytes(b->n_tiles));
   for (int k = 0; k < nsteps; k++) {
-    fused_step_kernel<T, TY, TX, FAST><<<grid, kNT, sizeof(S), st>>>(b->instances, b->tile_instance,
-                                                                b->n_tiles, parts, bct);
+    fused_step_kernel<T, TY, TX, FAST><<<grid, kNT, sizeof(S), st>>>(
+        b->instances, b->tile_instance, b->n_tiles, parts, bct);
   }
   return check_launch("hb_fused_step");
+}
+
+template <typename T, int TY, bool FAST = (sizeof(T) == 4)>
+int launch_rows(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
+  using S = RowsSmem<T, TY>;
+  static std::once_flag once;
+  static cudaError_t attr_err = cudaSuccess;
+  static int blocks_per_sm = 1;
+  std::call_once(once, [] {
+    attr_err = cudaFuncSetAttribute(rows_step_kernel<T, TY, FAST>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(S));
+    if (attr_err == cudaSuccess)
+      attr_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &blocks_per_sm, rows_step_kernel<T, TY, FAST>, kRowsNT, sizeof(S));
+    if (blocks_per_sm < 1) blocks_per_sm = 1;
+  });
+  if (attr_err != cudaSuccess)
+    return set_error(HB_ERR_CUDA, "fused step setup: %s", cudaGetErrorString(attr_err));
+  int grid = b->grid_blocks > 0 ? b->grid_blocks : blocks_per_sm * num_sms();
+  if (grid > b->n_tiles) grid = b->n_tiles;
+  char *ws = reinterpret_cast<char *>(b->workspace);
+  TilePartial *parts = reinterpret_cast<TilePartial *>(ws);
+  BcTable *bct = reinterpret_cast<BcTable *>(ws + ws_partials_bytes(b->n_tiles));
+  const CUtensorMap *maps = reinterpret_cast<const CUtensorMap *>(ws + ws_maps_offset(b));
+  for (int k = 0; k < nsteps; k++) {
+    rows_step_kernel<T, TY, FAST><<<grid, kRowsNT, sizeof(S), st>>>(
+        b->instances, b->tile_instance, b->n_tiles, parts, bct, maps);
+  }
+  return check_launch("hb_fused_step");
+}
+
+bool uses_rows_kernel(const hb_fused_batch *b) { return !(b->flags & HB_FLAG_TILE_TASKS); }
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+int encode_2d(CUtensorMap *map, CUtensorMapDataType dt, size_t esize, const void *base,
+              uint64_t width, uint64_t rows, uint32_t box_w, uint32_t box_h) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return set_error(HB_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+  if (((uintptr_t)base & 15) != 0)
+    return set_error(HB_ERR_ARG, "tensor base address must be 16-byte aligned");
+  if ((width * esize) % 16 != 0 || (box_w * esize) % 16 != 0)
+    return set_error(HB_ERR_ARG, "tensor row pitch and box width must be multiples of 16 bytes");
+  cuuint64_t dims[2] = {width, rows};
+  cuuint64_t strides[1] = {width * esize};
+  cuuint32_t box[2] = {box_w, box_h};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map, dt, 2, const_cast<void *>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(HB_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return HB_OK;
+}
+
+// Tensor maps of every instance for the rows kernel (box heights depend on
+// the tile height).  Host records are read from b->instances_host.
+int encode_maps(const hb_fused_batch *b, cudaStream_t st) {
+  if (!b->instances_host) return set_error(HB_ERR_ARG, "hb_fused_prepare: instances_host is null");
+  const int TY = b->tile_y;
+  const size_t es = b->dtype == HB_F64 ? 8 : 4;
+  const CUtensorMapDataType dt =
+      b->dtype == HB_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  std::vector<CUtensorMap> maps((size_t)b->n_instances * kMapsPerInstance);
+  for (int i = 0; i < b->n_instances; i++) {
+    const hb_instance &in = b->instances_host[i];
+    const uint64_t rows_s = (uint64_t)((in.rows + 63) / 64 * 64 + 2 * HB_PAD_Y);
+    if ((int64_t)in.tiles_y * TY + 4 > (int64_t)rows_s || in.tiles_x * kTW + 8 > in.pitch)
+      return set_error(HB_ERR_ARG, "instance %d: storage smaller than its tiles", i);
+    CUtensorMap *m = &maps[(size_t)i * kMapsPerInstance];
+    const void *srcs[7] = {in.h[0], in.h[1], in.qx[0], in.qx[1], in.qy[0], in.qy[1], in.z};
+    for (int k = 0; k < 7; k++) {
+      int rc = encode_2d(&m[k], dt, es, srcs[k], (uint64_t)in.pitch, rows_s, kSWF, TY + 4);
+      if (rc) return rc;
+    }
+    int rc = encode_2d(&m[7], dt, es, in.h_max, (uint64_t)in.pitch, rows_s, kTW, TY);
+    if (rc) return rc;
+    rc = encode_2d(&m[8], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, in.code, (uint64_t)in.code_pitch,
+                   rows_s, kSWC, TY + 4);
+    if (rc) return rc;
+  }
+  char *dst = reinterpret_cast<char *>(b->workspace) + ws_maps_offset(b);
+  cudaError_t e = cudaMemcpyAsync(dst, maps.data(), maps.size() * sizeof(CUtensorMap),
+                                  cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return set_error(HB_ERR_CUDA, "tensor maps upload: %s", cudaGetErrorString(e));
+  return HB_OK;
 }
 
 }  // namespace
@@ -719,7 +1448,7 @@ using namespace hb;
 
 extern "C" size_t hb_fused_workspace_size(const hb_fused_batch *b) {
   if (!b) return 0;
-  return ws_partials_bytes(b->n_tiles) + (size_t)b->n_instances * sizeof(BcTable);
+  return ws_maps_offset(b) + (size_t)b->n_instances * kMapsPerInstance * sizeof(CUtensorMap);
 }
 
 extern "C" int hb_fused_prepare(const hb_fused_batch *b, void *stream) {
@@ -728,6 +1457,12 @@ extern "C" int hb_fused_prepare(const hb_fused_batch *b, void *stream) {
   if (b->dtype != HB_F32 && b->dtype != HB_F64)
     return set_error(HB_ERR_ARG, "hb_fused_prepare: bad dtype %d", b->dtype);
   auto st = as_stream(stream);
+  if (uses_rows_kernel(b)) {
+    if (b->tile_x != kTW || (b->tile_y != 32 && b->tile_y != 64))
+      return set_error(HB_ERR_ARG, "hb_fused_prepare: rows kernel tiles are 32 wide, 32 or 64 high");
+    int rc = encode_maps(b, st);
+    if (rc) return rc;
+  }
   BcTable *bct = reinterpret_cast<BcTable *>((char *)b->workspace + ws_partials_bytes(b->n_tiles));
   if (b->dtype == HB_F64)
     prepare_kernel<double><<<b->n_instances, kNT, 0, st>>>(b->instances, bct);
@@ -744,21 +1479,25 @@ extern "C" int hb_fused_step(const hb_fused_batch *b, int nsteps, void *stream) 
   if (nsteps == 0) return HB_OK;
   auto st = as_stream(stream);
   const int ty = b->tile_y, tx = b->tile_x;
-  if (b->dtype == HB_F32 && (b->flags & HB_FLAG_EXACT_FP32)) {
+  const bool exact = (b->flags & HB_FLAG_EXACT_FP32) != 0;
+  if (uses_rows_kernel(b)) {
+    if (tx != kTW) return set_error(HB_ERR_ARG, "hb_fused_step: rows kernel tiles are 32 wide");
+    if (b->dtype == HB_F32 && exact) {
+      if (ty == 32) return launch_rows<float, 32, false>(b, nsteps, st);
+    } else if (b->dtype == HB_F32) {
+      if (ty == 32) return launch_rows<float, 32>(b, nsteps, st);
+      if (ty == 64) return launch_rows<float, 64>(b, nsteps, st);
+    } else if (b->dtype == HB_F64) {
+      if (ty == 32) return launch_rows<double, 32>(b, nsteps, st);
+    }
+    return set_error(HB_ERR_ARG, "hb_fused_step: rows kernel %dx%d not built for this dtype", ty, tx);
+  }
+  if (b->dtype == HB_F32 && exact) {
     if (ty == 32 && tx == 32) return launch_steps<float, 32, 32, false>(b, nsteps, st);
-    return set_error(HB_ERR_ARG, "hb_fused_step: exact FP32 tile %dx%d not built", ty, tx);
-  }
-  if (b->dtype == HB_F32) {
+  } else if (b->dtype == HB_F32) {
     if (ty == 32 && tx == 32) return launch_steps<float, 32, 32>(b, nsteps, st);
-    if (ty == 16 && tx == 64) return launch_steps<float, 16, 64>(b, nsteps, st);
-    if (ty == 16 && tx == 32) return launch_steps<float, 16, 32>(b, nsteps, st);
-    if (ty == 8 && tx == 64) return launch_steps<float, 8, 64>(b, nsteps, st);
-    return set_error(HB_ERR_ARG, "hb_fused_step: FP32 tile %dx%d not built", ty, tx);
-  }
-  if (b->dtype == HB_F64) {
+  } else if (b->dtype == HB_F64) {
     if (ty == 32 && tx == 32) return launch_steps<double, 32, 32>(b, nsteps, st);
-    if (ty == 16 && tx == 32) return launch_steps<double, 16, 32>(b, nsteps, st);
-    return set_error(HB_ERR_ARG, "hb_fused_step: FP64 tile %dx%d not built", ty, tx);
   }
-  return set_error(HB_ERR_ARG, "hb_fused_step: bad dtype %d", b->dtype);
+  return set_error(HB_ERR_ARG, "hb_fused_step: tile-task kernel %dx%d not built", ty, tx);
 }

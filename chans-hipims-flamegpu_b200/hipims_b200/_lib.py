@@ -70,6 +70,7 @@ class HbFusedBatch(ctypes.Structure):
         ("dtype", c_i32), ("n_instances", c_i32), ("n_tiles", c_i32), ("tile_y", c_i32),
         ("tile_x", c_i32), ("grid_blocks", c_i32), ("order", c_i32), ("flags", c_i32),
         ("instances", c_vp), ("tile_instance", c_vp), ("workspace", c_vp),
+        ("instances_host", c_vp),
     ]
 
 

@@ -37,6 +37,9 @@ extern "C" {
 /* hb_fused_batch.flags: FP32 with the reference's operation forms (no
  * approximate division/square root, no algebraic shortcuts). */
 #define HB_FLAG_EXACT_FP32 1
+/* hb_fused_batch.flags: use the face-task kernel (any 32x32 tile, staged by
+ * plain loads) instead of the row-walking kernel (32-wide tiles staged by TMA). */
+#define HB_FLAG_TILE_TASKS 2
 
 /* Per-instance control block, device memory.  Written by hb_fused_prepare
  * and by the last tile of every step; read by the host between launches. */
@@ -99,13 +102,14 @@ typedef struct hb_fused_batch {
   int32_t dtype;             /* HB_F32 or HB_F64 */
   int32_t n_instances;
   int32_t n_tiles;           /* sum of tiles_x * tiles_y */
-  int32_t tile_y, tile_x;    /* tile shape: 8, 16, 32 or 64 each */
+  int32_t tile_y, tile_x;    /* tile shape: 32 wide, 32 or 64 high */
   int32_t grid_blocks;       /* 0: one wave of resident blocks */
   int32_t order;             /* 2 (MUSCL); 1 (bed-only minmod) */
   int32_t flags;             /* HB_FLAG_* bits */
   const hb_instance *instances;  /* device [n_instances] */
   const int32_t *tile_instance;  /* device [n_tiles] */
   void *workspace;               /* device, hb_fused_workspace_size() bytes */
+  const hb_instance *instances_host; /* host copy of instances (hb_fused_prepare) */
 } hb_fused_batch;
 
 #ifdef __cplusplus

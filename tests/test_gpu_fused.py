@@ -29,15 +29,16 @@ def compare(fs, sim, k=0):
     return {f: float(np.abs(got[f] - st[f]).max()) for f in ("h", "qx", "qy", "h_max")}
 
 
-@pytest.mark.parametrize("tile", [(32, 32), (16, 32)])
-def test_fused_fp64_dam_break(cuda, tile):
+@pytest.mark.parametrize("kernel", ["rows", "tasks"])
+def test_fused_fp64_dam_break(cuda, kernel):
     from hipims_b200 import scenarios as S
     from hipims_b200.fused import FusedSolver
 
     d = S.dam_break(100)
     sim = O.Sim(d, order=2)
     sim.run(300)
-    fs = FusedSolver(catchment(d), dtype=torch.float64, tile=tile, device=cuda)
+    fs = FusedSolver(catchment(d), dtype=torch.float64, tile=(32, 32), device=cuda,
+                     kernel=kernel)
     fs.step(300)
     c = fs.controls()[0]
     assert c.step == 300
@@ -54,7 +55,8 @@ def test_fused_fp64_channel_boundaries(cuda):
     d = S.channel()
     sim = O.Sim(d, order=2)
     n = sim.run(100000, d["t_end"])
-    fs = FusedSolver(catchment(d, t_end=d["t_end"]), dtype=torch.float64, device=cuda)
+    fs = FusedSolver(catchment(d, t_end=d["t_end"]), dtype=torch.float64, tile=(32, 32),
+                     device=cuda)
     fs.step(n + 5)
     c = fs.controls()[0]
     assert c.step == n and c.halted
@@ -71,7 +73,8 @@ def test_fused_fp64_mixed_boundaries_uniform_rain(cuda, seed):
     d["rain"] = np.array([[0.0, 2e-4], [1.0, 5e-4], [10.0, 0.0]])
     sim = O.Sim(d, order=2, export_step=0.75)
     sim.run(60)
-    fs = FusedSolver(catchment(d, export_step=0.75), dtype=torch.float64, device=cuda)
+    fs = FusedSolver(catchment(d, export_step=0.75), dtype=torch.float64, tile=(32, 32),
+                     device=cuda)
     fs.step(60)
     c = fs.controls()[0]
     assert c.exports == sim.g.exports and c.t == pytest.approx(sim.t, rel=1e-12)
@@ -79,18 +82,23 @@ def test_fused_fp64_mixed_boundaries_uniform_rain(cuda, seed):
     assert max(err.values()) < 1e-10, err
 
 
-def test_fused_fp32_dam_break_1000_steps(cuda):
-    """Config 1 (256 x 256, 1000 steps) in FP32 vs the FP64 oracle."""
+@pytest.mark.parametrize("tile,kernel", [((64, 32), "rows"), ((32, 32), "rows"),
+                                         ((32, 32), "tasks")])
+def test_fused_fp32_dam_break_1000_steps(cuda, tile, kernel):
+    """Config 1 (256 x 256, 1000 steps) in FP32 vs the FP64 oracle.  The
+    problem is uniform along y, so qy must stay exactly 0."""
     from hipims_b200 import scenarios as S
     from hipims_b200.fused import FusedSolver
 
     d = S.dam_break(256)
     sim = O.Sim(d, order=2)
     dts = sim.run_record(1000)
-    fs = FusedSolver(catchment(d, dt_replay=dts), dtype=torch.float32, device=cuda)
+    fs = FusedSolver(catchment(d, dt_replay=dts), dtype=torch.float32, tile=tile, device=cuda,
+                     kernel=kernel)
     fs.step(1000)
     err = compare(fs, sim)
-    print("FP32 fused vs FP64 oracle (replayed dt), 1000 steps:", err)
+    print("FP32 fused vs FP64 oracle (replayed dt), 1000 steps:", tile, kernel, err)
+    assert np.abs(fs.compacted()["qy"]).max() == 0.0
     assert err["h"] <= 1e-4
     # adaptive FP32 dt stays within round-off of the FP64 schedule
     fa = FusedSolver(catchment(d), dtype=torch.float32, device=cuda)
