@@ -143,7 +143,10 @@ flux_kernel(int64_t M, int64_t N, const int32_t *__restrict__ wet,
   qy_flux[i] = fqy;
 }
 
-// Implicit Manning friction + Euler update, zeroing the accumulators.
+// Implicit Manning friction + Euler update, zeroing the accumulators.  The
+// reference kernel writes this step with double literals, so its FP32 build
+// evaluates C_f and the implicit update in double; D below reproduces those
+// promotions (for T = double it changes nothing).
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 friction_update_kernel(int64_t M, const int32_t *__restrict__ wet, T *__restrict__ hu,
@@ -152,6 +155,7 @@ friction_update_kernel(int64_t M, const int32_t *__restrict__ wet, T *__restrict
                        T *__restrict__ wlp, T *__restrict__ qxp, T *__restrict__ qyp,
                        T *__restrict__ zp, const T *__restrict__ manning,
                        const T *__restrict__ dtp) {
+  using D = double;
   int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= M) return;
   const T hs = T(kHSmall), g = T(kG), dt = dtp[0];
@@ -163,29 +167,31 @@ friction_update_kernel(int64_t M, const int32_t *__restrict__ wet, T *__restrict
     qy = T(0);
   } else {
     const T n = manning[landuse[i]];
-    const T C_f = g * n * n * pow(h, T(-1.0 / 3.0));
+    const T C_f = (T)((D)(g * n * n) * pow((D)h, -1.0 / 3.0));
     qx += qxu[i];
     qy += qyu[i];
     const T q_norm = sqrt(qx * qx + qy * qy);
+    const T h2 = h * h;
+    const D lim = 5.0 * (D)h * (D)sqrt(h * g);
     if (n > T(0)) {
       if (fabs(qx) > T(1.0e-10)) {
-        T temp = (T(1) - sqrt(T(1) + (T(4) * dt * C_f) / (h * h) * q_norm)) /
-                 (T(-2) * dt * C_f / (h * h) * (q_norm / qx));
-        if (fabs(temp) > T(5) * h * sqrt(h * g)) {
-          qx = T(2) * temp - qx;
-          if (qx * temp <= T(0)) qx = T(0);
+        const D temp = (1.0 - sqrt(1.0 + (4.0 * (D)dt * (D)C_f) / (D)h2 * (D)q_norm)) /
+                       (-2.0 * (D)dt * (D)C_f / (D)h2 * (D)(q_norm / qx));
+        if (fabs(temp) > lim) {
+          qx = (T)(2.0 * temp - (D)qx);
+          if ((D)qx * temp <= 0.0) qx = T(0);
         } else {
-          qx = temp;
+          qx = (T)temp;
         }
       }
       if (fabs(qy) > T(1.0e-10)) {
-        T temp = (T(1) - sqrt(T(1) + (T(4) * dt * C_f) / (h * h) * q_norm)) /
-                 (T(-2) * dt * C_f / (h * h) * (q_norm / qy));
-        if (fabs(temp) > T(5) * h * sqrt(h * g)) {
-          qy = T(2) * temp - qy;
-          if (qy * temp <= T(0)) qy = T(0);
+        const D temp = (1.0 - sqrt(1.0 + (4.0 * (D)dt * (D)C_f) / (D)h2 * (D)q_norm)) /
+                       (-2.0 * (D)dt * (D)C_f / (D)h2 * (D)(q_norm / qy));
+        if (fabs(temp) > lim) {
+          qy = (T)(2.0 * temp - (D)qy);
+          if ((D)qy * temp <= 0.0) qy = T(0);
         } else {
-          qy = temp;
+          qy = (T)temp;
         }
       }
     }

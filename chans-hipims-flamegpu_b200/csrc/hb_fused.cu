@@ -810,13 +810,26 @@ __device__ __forceinline__ Cell<T> edge_of(const Cell<T> &c, const Slope<T> &s, 
 }
 
 // Face between valid cells A (west/south) and B (east/north) from A's side,
-// given both MUSCL edge states.  DIR 0: normal +x; DIR 1: normal +y.
+// from the cells and their MUSCL slopes along DIR (0: normal +x, 1: +y).
+// FAST (FP32) evaluates the face with bed elevations measured from A's bed:
+// every operation of the scheme is invariant under a common shift of z, and
+// in that frame eta = h + z is rounded at the scale of the local relief
+// instead of the absolute elevation.
 template <typename T, bool FAST, int DIR>
-__device__ __forceinline__ FaceOut<T> face_edges(const Cell<T> &A, const Cell<T> &B,
-                                                 Cell<T> eL, Cell<T> eR) {
+__device__ __forceinline__ FaceOut<T> face_edges(Cell<T> A, Cell<T> B, const Slope<T> &sA,
+                                                 const Slope<T> &sB) {
   const T hs = T(kHSmall), g = T(kG);
   FaceOut<T> o{T(0), T(0), T(0), T(0), T(0)};
   if (A.h < hs && B.h < hs) return o;
+  if constexpr (FAST) {
+    const T zref = A.z;
+    A.z = T(0);
+    B.z = B.z - zref;
+    A.wl = A.h;
+    B.wl = B.z + B.h;
+  }
+  Cell<T> eL = edge_of(A, sA, T(1));
+  Cell<T> eR = edge_of(B, sB, T(-1));
   T ux_l, uy_l, ux_r, uy_r;
   if constexpr (FAST) {
     const T il = eL.h < hs ? T(0) : T(1) / eL.h;
@@ -855,10 +868,17 @@ __device__ __noinline__ void ghost_face(const Cell<T> C, int cls, int type, cons
   Cell<T> G;
   const T hb = (T)bcv[0], wlb = (T)(bcv[1] - (double)datum);
   const T qxb = (T)bcv[2], qyb = (T)bcv[3];
-  if (!ghost(type, false, C, n0, n1, hb, wlb, qxb, qyb, G)) return;
+  Cell<T> Cl = C;
+  T wlbl = wlb;
+  if constexpr (FAST) {  // bed measured from C's bed, as for interior faces
+    wlbl = wlb - C.z;
+    Cl.z = T(0);
+    Cl.wl = Cl.h;
+  }
+  if (!ghost(type, false, Cl, n0, n1, hb, wlbl, qxb, qyb, G)) return;
   (void)cls;
-  if (C.h < hs && G.h < hs) return;
-  Cell<T> eL = C, eR = G;
+  if (Cl.h < hs && G.h < hs) return;
+  Cell<T> eL = Cl, eR = G;
   T ux_l, uy_l, ux_r, uy_r;
   if constexpr (FAST) {
     const T il = eL.h < hs ? T(0) : T(1) / eL.h;
@@ -871,7 +891,7 @@ __device__ __noinline__ void ghost_face(const Cell<T> C, int cls, int type, cons
     ux_r = eR.h < hs ? T(0) : eR.qx / eR.h;
     uy_r = eR.h < hs ? T(0) : eR.qy / eR.h;
   }
-  hydro2(C.wl, G.wl, eL, eR);
+  hydro2(Cl.wl, G.wl, eL, eR);
   const T u_L = ux_l * n0 + uy_l * n1, u_R = ux_r * n0 + uy_r * n1;
   const T v_L = -ux_l * n1 + uy_l * n0, v_R = -ux_r * n1 + uy_r * n0;
   T Fh, Fn, Ft;
@@ -880,7 +900,7 @@ __device__ __noinline__ void ghost_face(const Cell<T> C, int cls, int type, cons
     out[1] = Fn * n0 + Ft * (-n1);
     out[2] = Fn * n1 + Ft * n0;
   }
-  out[3] = T(0.5) * g * (C.h + eL.h) * (eL.z - C.z);
+  out[3] = T(0.5) * g * (Cl.h + eL.h) * (eL.z - Cl.z);
 }
 
 template <typename T, int TY>
@@ -903,13 +923,13 @@ struct RowsView {
 };
 
 // Face between A (minus side) and B (plus side) along DIR, any validity.
-// eA / eB: MUSCL edges (used only when both are valid).
+// sA / sB: MUSCL slopes of A and B along DIR (used only when both are valid).
 template <typename T, bool FAST, int DIR, int TY>
 __device__ __forceinline__ FaceOut<T> face_any(const RowsSmem<T, TY> &s, const Cell<T> &A,
                                                uint8_t ca, const Cell<T> &B, uint8_t cb,
-                                               const Cell<T> &eA, const Cell<T> &eB, T datum) {
+                                               const Slope<T> &sA, const Slope<T> &sB, T datum) {
   const bool va = is_valid(ca), vb = is_valid(cb);
-  if (va && vb) return face_edges<T, FAST, DIR>(A, B, eA, eB);
+  if (va && vb) return face_edges<T, FAST, DIR>(A, B, sA, sB);
   FaceOut<T> o{T(0), T(0), T(0), T(0), T(0)};
   const T n0 = DIR == 0 ? T(1) : T(0), n1 = DIR == 0 ? T(0) : T(1);
   T out[4];
@@ -1037,8 +1057,7 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
       const uint8_t ca = V.code(i, 31), cb = V.code(i, 32);
       const Slope<T> sa = slope_of(a, V.cell(i, 30), is_valid(V.code(i, 30)), b, is_valid(cb));
       const Slope<T> sb = slope_of(b, a, is_valid(ca), V.cell(i, 33), is_valid(V.code(i, 33)));
-      const FaceOut<T> f = face_any<T, FAST, 0>(s, a, ca, b, cb, edge_of(a, sa, T(1)),
-                                                edge_of(b, sb, T(-1)), datum_tile);
+      const FaceOut<T> f = face_any<T, FAST, 0>(s, a, ca, b, cb, sa, sb, datum_tile);
       s.xe[w][lane][0] = f.fh;
       s.xe[w][lane][1] = f.fx;
       s.xe[w][lane][2] = f.fy;
@@ -1062,8 +1081,7 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
       syC = slope_of(cC, cS, is_valid(kS), cN, is_valid(kN));
       syS = slope_of(cS, cSS, is_valid(kSS), cC, is_valid(kC));
       // face between rows r0-1 (north) and r0 (south), from the south side
-      nf = face_any<T, FAST, 1>(s, cC, kC, cN, kN, edge_of(cC, syC, T(1)),
-                                edge_of(cN, syN, T(-1)), datum_tile);
+      nf = face_any<T, FAST, 1>(s, cC, kC, cN, kN, syC, syN, datum_tile);
     }
     double vol = 0.0, outf = 0.0, smax = 0.0;
     int any_dry = 0;
@@ -1091,8 +1109,7 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
         sxW.qy = s.sxw[w][i - r0][3];
       }
       // west face (this cell is B) -> the west neighbour's east face
-      const FaceOut<T> wf = face_any<T, FAST, 0>(s, cW, kW, cC, kC, edge_of(cW, sxW, T(1)),
-                                                 edge_of(cC, sxC, T(-1)), datum_tile);
+      const FaceOut<T> wf = face_any<T, FAST, 0>(s, cW, kW, cC, kC, sxW, sxC, datum_tile);
       T ef_h = __shfl_down_sync(0xffffffffu, wf.fh, 1);
       T ef_x = __shfl_down_sync(0xffffffffu, wf.fx, 1);
       T ef_y = __shfl_down_sync(0xffffffffu, wf.fy, 1);
@@ -1104,8 +1121,7 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
         ef_a = s.xe[w][i - r0][3];
       }
       // south face (this cell is B, the row below is A)
-      const FaceOut<T> sf = face_any<T, FAST, 1>(s, cS, kS, cC, kC, edge_of(cS, syS, T(1)),
-                                                 edge_of(cC, syC, T(-1)), datum_tile);
+      const FaceOut<T> sf = face_any<T, FAST, 1>(s, cS, kS, cC, kC, syS, syC, datum_tile);
       const int ry = y0 + i;
       if (vC) {
         const T hc = cC.h;

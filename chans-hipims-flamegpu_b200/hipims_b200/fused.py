@@ -167,7 +167,7 @@ class FusedSolver:
     """Advance one or more catchments with the fused dense-tile kernel."""
 
     def __init__(self, catchments: Catchment | Sequence[Catchment], dtype=torch.float32,
-                 tile: tuple[int, int] = (64, 32), device="cuda", grid_blocks: int = 0,
+                 tile: tuple[int, int] | None = None, device="cuda", grid_blocks: int = 0,
                  exact_fp32: bool = False, kernel: str = "rows"):
         if isinstance(catchments, Catchment):
             catchments = [catchments]
@@ -175,6 +175,8 @@ class FusedSolver:
             raise ValueError("dtype must be float32 or float64")
         self.device = torch.device(device)
         self.dtype = dtype
+        if tile is None:  # rows kernel: 32 wide; 64 high in FP32, 32 high in FP64
+            tile = (64, 32) if dtype == torch.float32 and kernel == "rows" else (32, 32)
         self.tile = tuple(tile)
         self.inst = [_Instance(c, dtype, self.device, self.tile) for c in catchments]
         n = len(self.inst)

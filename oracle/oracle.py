@@ -250,12 +250,17 @@ class Sim:
     def dt(self) -> float:
         return self.g.dt
 
+    _steps = 0
+
     def step(self, n: int = 1) -> None:
         for _ in range(n):
             lib().or_godunov_step(ctypes.byref(self.g))
+        self._steps += n
 
     def run(self, n: int, t_end: float = float("inf")) -> int:
-        return int(lib().or_godunov_run(ctypes.byref(self.g), int(n), float(t_end)))
+        k = int(lib().or_godunov_run(ctypes.byref(self.g), int(n), float(t_end)))
+        self._steps += k
+        return k
 
     def run_record(self, n: int, t_end: float = float("inf")) -> np.ndarray:
         """Step n times (or to t_end); return the dt chosen after each step."""
@@ -264,6 +269,7 @@ class Sim:
             if not self.g.t < t_end:
                 break
             lib().or_godunov_step(ctypes.byref(self.g))
+            self._steps += 1
             dts.append(self.g.dt)
         return np.asarray(dts)
 
