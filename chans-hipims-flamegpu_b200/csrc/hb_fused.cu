@@ -945,8 +945,8 @@ __device__ __forceinline__ FaceOut<T> face_any(const RowsSmem<T, TY> &s, const C
   return o;
 }
 
-template <typename T, int TY, bool FAST>
-__global__ void __launch_bounds__(kRowsNT)
+template <typename T, int TY, bool FAST, int MINB>
+__global__ void __launch_bounds__(kRowsNT, MINB)
 rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restrict__ tile_inst,
                  int n_tiles, TilePartial *__restrict__ partials, BcTable *__restrict__ bct,
                  const CUtensorMap *__restrict__ maps) {
@@ -1354,18 +1354,18 @@ int launch_steps(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   return check_launch("hb_fused_step");
 }
 
-template <typename T, int TY, bool FAST = (sizeof(T) == 4)>
+template <typename T, int TY, bool FAST = (sizeof(T) == 4), int MINB = 1>
 int launch_rows(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   using S = RowsSmem<T, TY>;
   static std::once_flag once;
   static cudaError_t attr_err = cudaSuccess;
   static int blocks_per_sm = 1;
   std::call_once(once, [] {
-    attr_err = cudaFuncSetAttribute(rows_step_kernel<T, TY, FAST>,
+    attr_err = cudaFuncSetAttribute(rows_step_kernel<T, TY, FAST, MINB>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(S));
     if (attr_err == cudaSuccess)
       attr_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &blocks_per_sm, rows_step_kernel<T, TY, FAST>, kRowsNT, sizeof(S));
+          &blocks_per_sm, rows_step_kernel<T, TY, FAST, MINB>, kRowsNT, sizeof(S));
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   });
   if (attr_err != cudaSuccess)
@@ -1377,7 +1377,7 @@ int launch_rows(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   BcTable *bct = reinterpret_cast<BcTable *>(ws + ws_partials_bytes(b->n_tiles));
   const CUtensorMap *maps = reinterpret_cast<const CUtensorMap *>(ws + ws_maps_offset(b));
   for (int k = 0; k < nsteps; k++) {
-    rows_step_kernel<T, TY, FAST><<<grid, kRowsNT, sizeof(S), st>>>(
+    rows_step_kernel<T, TY, FAST, MINB><<<grid, kRowsNT, sizeof(S), st>>>(
         b->instances, b->tile_instance, b->n_tiles, parts, bct, maps);
   }
   return check_launch("hb_fused_step");
@@ -1501,8 +1501,13 @@ extern "C" int hb_fused_step(const hb_fused_batch *b, int nsteps, void *stream) 
     if (b->dtype == HB_F32 && exact) {
       if (ty == 32) return launch_rows<float, 32, false>(b, nsteps, st);
     } else if (b->dtype == HB_F32) {
-      if (ty == 32) return launch_rows<float, 32>(b, nsteps, st);
-      if (ty == 64) return launch_rows<float, 64>(b, nsteps, st);
+      // register cap by resident CTAs per SM (flags bits 8-11)
+      const int minb = (b->flags >> HB_FLAG_MINB_SHIFT) & 0xF;
+      if (ty == 32 && minb == 0) return launch_rows<float, 32>(b, nsteps, st);
+      if (ty == 32 && minb == 5) return launch_rows<float, 32, true, 5>(b, nsteps, st);
+      if (ty == 32 && minb == 6) return launch_rows<float, 32, true, 6>(b, nsteps, st);
+      if (ty == 64 && minb == 0) return launch_rows<float, 64>(b, nsteps, st);
+      if (ty == 64 && minb == 4) return launch_rows<float, 64, true, 4>(b, nsteps, st);
     } else if (b->dtype == HB_F64) {
       if (ty == 32) return launch_rows<double, 32>(b, nsteps, st);
     }

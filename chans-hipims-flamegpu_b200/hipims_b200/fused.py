@@ -168,7 +168,7 @@ class FusedSolver:
 
     def __init__(self, catchments: Catchment | Sequence[Catchment], dtype=torch.float32,
                  tile: tuple[int, int] | None = None, device="cuda", grid_blocks: int = 0,
-                 exact_fp32: bool = False, kernel: str = "rows"):
+                 exact_fp32: bool = False, kernel: str = "rows", minb: int = 0):
         if isinstance(catchments, Catchment):
             catchments = [catchments]
         if dtype not in (torch.float32, torch.float64):
@@ -242,7 +242,7 @@ class FusedSolver:
         b.tile_y, b.tile_x = self.tile
         b.grid_blocks = grid_blocks
         b.order = 2
-        b.flags = (1 if exact_fp32 else 0) | (2 if kernel == "tasks" else 0)
+        b.flags = (1 if exact_fp32 else 0) | (2 if kernel == "tasks" else 0) | (minb << 8)
         b.instances_host = ctypes.addressof(self._recs_host)
         b.instances = self.records.data_ptr()
         b.tile_instance = self.tile_instance.data_ptr()
