@@ -260,6 +260,15 @@ def run_ours(args) -> None:
         }
         if args.accuracy:
             line["accuracy"] = accuracy_vs_fp64(d, dev, SPINUP + args.warmup + args.steps)
+        if args.plain and world == 1:
+            pl = plain_fp64_rate(d, dev)
+            pl["fused_fp32_over_plain"] = value / pl["value"]
+            line["fp64_plain"] = pl
+        if args.ensemble and world == 1:
+            en = ensemble_rate(dev, args.ensemble_steps)
+            if "fp64_plain" in line:
+                en["over_plain_fp64"] = en["value"] / line["fp64_plain"]["value"]
+            line["ensemble"] = en
         if args.cpu_baseline and world == 1:
             line["cpu_baseline"] = {k: v for k, v in cpu_reference_rate(
                 d, args.cpu_steps, 0).items() if k in ("value", "unit", "cores", "kind",
@@ -269,6 +278,70 @@ def run_ours(args) -> None:
         dist.barrier()
         dist.destroy_process_group()
     del _lib
+
+
+def plain_fp64_rate(d: dict, dev, steps: int = 5) -> dict:
+    """The plain FP64 GPU path: the reference solver loop (Godunov object API,
+    compacted cells, gather-based per-cell fluxes, host syncs per step) on the
+    compat ops, on the same catchment, wall-clock per step."""
+    from hipims_b200.solver import Godunov
+
+    g = Godunov(dev, d["dx"], d["cfl"], 1.0e30, secondOrder=True,
+                firstTimeStep=d["first_dt"], tensorType=torch.float64)
+    g._export_enabled = False
+    T = lambda a: torch.as_tensor(np.asarray(a, dtype=np.float64))
+    mask = torch.as_tensor(d["mask"])
+    g.init__fluidField_tensor(mask, T(d["h"]), T(d["qx"]), T(d["qy"]), T(d["wl"]), T(d["z"]),
+                              dev)
+    g.set__frictionField_tensor(torch.tensor(d["manning"], dtype=torch.float64, device=dev), dev)
+    g.set_landuse(mask, torch.as_tensor(d["landuse"]), dev)
+    g.set_distributed_rainfall_station_Mask(mask, torch.zeros(mask.shape, dtype=torch.int16), dev)
+
+    def one():
+        g.addFlux()
+        g.addStation_PrecipitationSource(d["rain"], dev)
+        g.time_friction_euler_update_cuda(dev)
+
+    for _ in range(SPINUP):
+        one()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one()
+    torch.cuda.synchronize(dev)
+    el = time.perf_counter() - t0
+    n = int(g._h_internal.numel())
+    return {"value": n * steps / el / 1e9, "unit": METRIC, "steps": steps, "dtype": "f64",
+            "path": "Godunov loop on the compat ops (reference kernel structure), wall clock"}
+
+
+def ensemble_rate(dev, steps: int, count: int = 64, seed: int = 0) -> dict:
+    """Config 3: `count` catchments (sides 256-1536, own hyetographs) advanced
+    together, one fused launch per step for all of them."""
+    from hipims_b200 import autotune, scenarios as S
+    from hipims_b200.fused import FusedSolver
+    from hipims_b200.scenarios import catchment_from
+
+    cs = [catchment_from(d) for d in S.ensemble(count, seed=seed)]
+    cfg = autotune.tune(cs, torch.float32, dev, steps=4)
+    fs = FusedSolver(cs, dtype=torch.float32, device=dev, tile=cfg["tile"],
+                     minb=cfg.get("minb", 0))
+    cells = sum(i.n_valid for i in fs.inst)
+    fs.step(SPINUP)
+    fs.capture(steps)
+    fs.replay()  # warm-up replay
+    st = torch.cuda.current_stream(dev)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    a.record(st)
+    fs.replay()
+    b.record(st)
+    torch.cuda.synchronize(dev)
+    ms = a.elapsed_time(b)
+    return {"value": cells * steps / (ms * 1e-3) / 1e9, "unit": METRIC, "instances": count,
+            "cells": cells, "steps": steps, "ms_per_step": ms / steps,
+            "launch": "one CUDA-graph replay of `steps` fused launches for all instances",
+            "tile": list(cfg["tile"]), "minb": cfg.get("minb", 0)}
 
 
 def accuracy_vs_fp64(d: dict, dev, steps: int) -> dict:
@@ -309,6 +382,9 @@ def main() -> None:
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-accuracy", dest="accuracy", action="store_false")
+    ap.add_argument("--no-plain", dest="plain", action="store_false")
+    ap.add_argument("--no-ensemble", dest="ensemble", action="store_false")
+    ap.add_argument("--ensemble-steps", type=int, default=20)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -721,6 +721,7 @@ struct RowsSmem {
   T sxw[kRowsNW][R][4];       // x-slope of col -1: h, z, qx, qy
   double bc[HB_MAX_CLASSES][4];
   int bctype[HB_MAX_CLASSES];
+  T manning[HB_MAX_ZONES];
   T ddatum[9];
   double red_d[2][kRowsNW];
   double red_s[kRowsNW];
@@ -994,7 +995,10 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
     if (tid < HB_MAX_CLASSES) {
       s.bctype[tid] = in.bc_type[tid];
       for (int q = 0; q < 4; q++) s.bc[tid][q] = bct[ii].v[tid][q];
+    } else if (tid >= 64 && tid < 64 + HB_MAX_ZONES) {
+      s.manning[tid - 64] = (T)in.manning[tid - 64];
     }
+    const int bug_y = in.bug_y, bug_x = in.bug_x;
     T datum_tile = T(0);
     if (in.datum) {
       const int by = y0 / HB_DATUM_BLOCK, bx = x0 / HB_DATUM_BLOCK;
@@ -1083,7 +1087,10 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
       // face between rows r0-1 (north) and r0 (south), from the south side
       nf = face_any<T, FAST, 1>(s, cC, kC, cN, kN, syC, syN, datum_tile);
     }
-    double vol = 0.0, outf = 0.0, smax = 0.0;
+    // per-thread partial sums over this warp's rows (<= 16 cells) in T; the
+    // tile and instance reductions are FP64
+    T vol_t = T(0), smax_t = T(0);
+    double outf = 0.0;
     int any_dry = 0;
     T *hout = (T *)in.h[1 - cur];
     T *qxout = (T *)in.qx[1 - cur];
@@ -1127,10 +1134,10 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
         const T hc = cC.h;
         bool active = first || hc > hs;
         if (!active) {
-          const bool bugE = (ry == in.bug_y && rx + 1 == in.bug_x);
-          const bool bugW = (ry == in.bug_y && rx - 1 == in.bug_x);
-          const bool bugN = (ry - 1 == in.bug_y && rx == in.bug_x);
-          const bool bugS = (ry + 1 == in.bug_y && rx == in.bug_x);
+          const bool bugE = (ry == bug_y && rx + 1 == bug_x);
+          const bool bugW = (ry == bug_y && rx - 1 == bug_x);
+          const bool bugN = (ry - 1 == bug_y && rx == bug_x);
+          const bool bugS = (ry + 1 == bug_y && rx == bug_x);
           active = (vE && !bugE && cE.h > hs) || (is_valid(kN) && !bugN && cN.h > hs) ||
                    (vW && !bugW && cW.h > hs) || (is_valid(kS) && !bugS && cS.h > hs);
         }
@@ -1173,17 +1180,18 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
         T h = hc + hu;
         T qx = cC.qx, qy = cC.qy;
         T sgh = T(0);
+        T ih = T(0);
         if (h < hs) {
           qx = T(0);
           qy = T(0);
         } else {
-          const T n = (T)in.manning[kC & 15];
+          const T n = s.manning[kC & 15];
           qx += qxu;
           qy += qyu;
           sgh = FAST ? (T)sqrtf((float)(g * h)) : (T)__fsqrt_rn((float)(g * h));
           if constexpr (FAST) {
+            ih = T(1) / h;
             if (n > T(0)) {
-              const T ih = T(1) / h;
               const T q_norm = sqrtf(qx * qx + qy * qy);
               const T a = dt * g * n * n * exp2f(-__log2f(h) * (T(1) / T(3))) * ih * ih;
               const T fct = T(2) / (T(1) + sqrtf(T(1) + T(4) * a * q_norm));
@@ -1240,11 +1248,14 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
         qyout[go] = qy;
         hmaxg[go] = fmax(h, s.hmax[i * kTW + j]);
         if (h > hs) {
-          smax = fmax(smax, (double)(sgh + fmax(fabs(qx), fabs(qy)) / h));
+          // CFL speed (HC/timeControl_Kernel.cu:186-189)
+          const T sp = FAST ? sgh + fmax(fabs(qx), fabs(qy)) * ih
+                            : sgh + fmax(fabs(qx), fabs(qy)) / h;
+          smax_t = fmax(smax_t, sp);
         } else {
           any_dry = 1;
         }
-        vol += (double)h;
+        vol_t += h;
       }
       // slide the column window down one row
       nf = sf;
@@ -1261,9 +1272,9 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
     }
 
     // --- tile partials and the instance's last-tile finalize
-    vol = warp_sum(vol);
+    double vol = warp_sum((double)vol_t);
     outf = warp_sum(outf);
-    smax = warp_max(smax);
+    double smax = warp_max((double)smax_t);
     any_dry = __any_sync(0xffffffffu, any_dry);
     if (lane == 0) {
       s.red_d[0][w] = vol;

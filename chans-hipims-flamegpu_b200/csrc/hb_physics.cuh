@@ -121,6 +121,23 @@ __device__ __forceinline__ bool hllc(T hL, T hR, T u_L, T u_R, T v_L, T v_R,
   T h_flux_R = qx_R;
   T qx_flux_R = u_R * qx_R + T(0.5) * g * hR * hR;
   T qy_flux_R = u_R * qy_R;
+  if constexpr (FAST) {
+    // branch-free region selection (same decisions as below; a NaN s_M
+    // selects the right state, as the reference's if-chain falls through)
+    const T s_M = fdiv<T, FAST>(s_L * hR * (u_R - s_R) - s_R * hL * (u_L - s_L),
+                                hR * (u_R - s_R) - hL * (u_L - s_L));
+    const T inv = T(1) / (s_R - s_L);
+    const T h_flux_M = (s_R * h_flux_L - s_L * h_flux_R + s_L * s_R * (hR - hL)) * inv;
+    const T qx_flux_M = (s_R * qx_flux_L - s_L * qx_flux_R + s_L * s_R * (qx_R - qx_L)) * inv;
+    const bool left = T(0) <= s_L;
+    const bool midL = !left && (s_L < T(0) && T(0) <= s_M);
+    const bool midR = !left && !midL && (s_M < T(0) && T(0) <= s_R);
+    const bool mid = midL || midR;
+    fh = left ? h_flux_L : (mid ? h_flux_M : h_flux_R);
+    fn = left ? qx_flux_L : (mid ? qx_flux_M : qx_flux_R);
+    ft = left ? qy_flux_L : (midL ? h_flux_M * v_L : (midR ? h_flux_M * v_R : qy_flux_R));
+    return true;
+  }
   if (T(0) <= s_L) {
     fh = h_flux_L;
     fn = qx_flux_L;
