@@ -1435,14 +1435,16 @@ int encode_2d(CUtensorMap *map, CUtensorMapDataType dt, size_t esize, const void
 }
 
 // Tensor maps of every instance for the rows kernel (box heights depend on
-// the tile height).  Host records are read from b->instances_host.
-int encode_maps(const hb_fused_batch *b, cudaStream_t st) {
+// the tile height), encoded into host_maps and copied to the workspace.
+// Host records are read from b->instances_host.
+int encode_maps(const hb_fused_batch *b, cudaStream_t st, CUtensorMap *host_maps) {
   if (!b->instances_host) return set_error(HB_ERR_ARG, "hb_fused_prepare: instances_host is null");
   const int TY = b->tile_y;
   const size_t es = b->dtype == HB_F64 ? 8 : 4;
   const CUtensorMapDataType dt =
       b->dtype == HB_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-  std::vector<CUtensorMap> maps((size_t)b->n_instances * kMapsPerInstance);
+  const size_t n_maps = (size_t)b->n_instances * kMapsPerInstance;
+  CUtensorMap *maps = host_maps;
   for (int i = 0; i < b->n_instances; i++) {
     const hb_instance &in = b->instances_host[i];
     const uint64_t rows_s = (uint64_t)((in.rows + 63) / 64 * 64 + 2 * HB_PAD_Y);
@@ -1461,7 +1463,7 @@ int encode_maps(const hb_fused_batch *b, cudaStream_t st) {
     if (rc) return rc;
   }
   char *dst = reinterpret_cast<char *>(b->workspace) + ws_maps_offset(b);
-  cudaError_t e = cudaMemcpyAsync(dst, maps.data(), maps.size() * sizeof(CUtensorMap),
+  cudaError_t e = cudaMemcpyAsync(dst, maps, n_maps * sizeof(CUtensorMap),
                                   cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return set_error(HB_ERR_CUDA, "tensor maps upload: %s", cudaGetErrorString(e));
@@ -1478,16 +1480,26 @@ extern "C" size_t hb_fused_workspace_size(const hb_fused_batch *b) {
   return ws_maps_offset(b) + (size_t)b->n_instances * kMapsPerInstance * sizeof(CUtensorMap);
 }
 
-extern "C" int hb_fused_prepare(const hb_fused_batch *b, void *stream) {
+namespace hb {
+namespace {
+
+// Prepare with tensor maps staged in host_maps (n_instances * 9 entries), or
+// in a temporary vector when host_maps is null.
+int prepare_impl(const hb_fused_batch *b, cudaStream_t st, CUtensorMap *host_maps) {
   if (!b || !b->instances || !b->workspace || b->n_instances <= 0)
     return set_error(HB_ERR_ARG, "hb_fused_prepare: bad batch record");
   if (b->dtype != HB_F32 && b->dtype != HB_F64)
     return set_error(HB_ERR_ARG, "hb_fused_prepare: bad dtype %d", b->dtype);
-  auto st = as_stream(stream);
   if (uses_rows_kernel(b)) {
     if (b->tile_x != kTW || (b->tile_y != 32 && b->tile_y != 64))
       return set_error(HB_ERR_ARG, "hb_fused_prepare: rows kernel tiles are 32 wide, 32 or 64 high");
-    int rc = encode_maps(b, st);
+    int rc;
+    if (host_maps) {
+      rc = encode_maps(b, st, host_maps);
+    } else {
+      std::vector<CUtensorMap> maps((size_t)b->n_instances * kMapsPerInstance);
+      rc = encode_maps(b, st, maps.data());
+    }
     if (rc) return rc;
   }
   BcTable *bct = reinterpret_cast<BcTable *>((char *)b->workspace + ws_partials_bytes(b->n_tiles));
@@ -1496,6 +1508,13 @@ extern "C" int hb_fused_prepare(const hb_fused_batch *b, void *stream) {
   else
     prepare_kernel<float><<<b->n_instances, kNT, 0, st>>>(b->instances, bct);
   return check_launch("hb_fused_prepare");
+}
+
+}  // namespace
+}  // namespace hb
+
+extern "C" int hb_fused_prepare(const hb_fused_batch *b, void *stream) {
+  return prepare_impl(b, as_stream(stream), nullptr);
 }
 
 extern "C" int hb_fused_step(const hb_fused_batch *b, int nsteps, void *stream) {
@@ -1532,4 +1551,70 @@ extern "C" int hb_fused_step(const hb_fused_batch *b, int nsteps, void *stream) 
     if (ty == 32 && tx == 32) return launch_steps<double, 32, 32>(b, nsteps, st);
   }
   return set_error(HB_ERR_ARG, "hb_fused_step: tile-task kernel %dx%d not built", ty, tx);
+}
+
+// ---------------------------------------------------------------------------
+// hb_fused_step_noalloc: the fused step with its scratch in this library's
+// own fixed device array instead of a caller-allocated workspace.
+//
+// The scratch (per-tile partial sums, boundary values, TMA descriptors) lives
+// in g_noalloc_scratch, kNoAllocScratchBytes per GPU that loads the library,
+// held until the process exits.  Host code must not pass g_noalloc_scratch to
+// a kernel directly: in host code that name is only a stand-in for the device
+// symbol.  Its device address is looked up once per device with
+// cudaGetSymbolAddress (on the first call on that device, which is why that
+// first call should come before any stream capture) and cached.
+// ---------------------------------------------------------------------------
+namespace hb {
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = (size_t)4 << 20;  // 4 MiB per GPU
+constexpr int kNoAllocMaxInstances = 256;
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[kMaxDevices];
+// host staging of the tensor maps (no heap allocation on this path)
+CUtensorMap g_noalloc_maps[kNoAllocMaxInstances * kMapsPerInstance];
+
+}  // namespace
+}  // namespace hb
+
+extern "C" int hb_fused_step_noalloc(const hb_fused_batch *b, int nsteps, int prepare,
+                                     void *stream) {
+  if (!b || !b->instances || !b->tile_instance || b->n_tiles <= 0 || b->n_instances <= 0)
+    return set_error(HB_ERR_ARG, "hb_fused_step_noalloc: bad batch record");
+  hb_fused_batch local = *b;
+  local.workspace = nullptr;
+  const size_t need = hb_fused_workspace_size(&local);
+  if (need > kNoAllocScratchBytes)
+    return set_error(HB_ERR_LIMIT,
+                     "hb_fused_step_noalloc: this batch needs %zu bytes of scratch; the fixed "
+                     "scratch holds %zu bytes (use hb_fused_step with a workspace)",
+                     need, kNoAllocScratchBytes);
+  if (b->n_instances > kNoAllocMaxInstances)
+    return set_error(HB_ERR_LIMIT, "hb_fused_step_noalloc: at most %d instances (got %d)",
+                     kNoAllocMaxInstances, b->n_instances);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return set_error(HB_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices)
+    return set_error(HB_ERR_LIMIT, "hb_fused_step_noalloc: device %d out of range", dev);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return set_error(HB_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = p;
+  }
+  local.workspace = g_noalloc_ptr[dev];
+  auto st = as_stream(stream);
+  if (prepare) {
+    int rc = prepare_impl(&local, st, g_noalloc_maps);
+    if (rc) return rc;
+  }
+  return hb_fused_step(&local, nsteps, stream);
 }

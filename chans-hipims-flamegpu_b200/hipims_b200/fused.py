@@ -270,6 +270,16 @@ class FusedSolver:
             _lib.check(_lib.lib().hb_fused_step(ctypes.byref(self.batch), int(nsteps),
                                                 self._stream()), "hb_fused_step")
 
+    def step_noalloc(self, nsteps: int = 1, prepare: bool = False) -> None:
+        """Enqueue nsteps steps through hb_fused_step_noalloc, which keeps its
+        scratch in the library's fixed device array instead of this solver's
+        workspace (for hosts that cannot allocate device memory).  Pass
+        prepare=True on the first such call."""
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.lib().hb_fused_step_noalloc(ctypes.byref(self.batch), int(nsteps),
+                                                        1 if prepare else 0, self._stream()),
+                       "hb_fused_step_noalloc")
+
     def capture(self, nsteps: int) -> None:
         """Capture nsteps steps in a CUDA graph for replay()."""
         self._graph = None

@@ -131,6 +131,29 @@ int hb_fused_prepare(const struct hb_fused_batch *batch, void *stream);
 /* Enqueue `nsteps` fused steps (graph-capturable; no host sync). */
 int hb_fused_step(const struct hb_fused_batch *batch, int nsteps, void *stream);
 
+/* Allocation-free variant of hb_fused_step (no counterpart in the reference).
+ * For callers that must not allocate device memory: host programs that own a
+ * fixed device-memory budget and manage it themselves (the FLAMEGPU agent
+ * runtime preallocates its buffers), and threads that cannot afford the
+ * device-wide synchronisation cudaMalloc/cudaFree can cause while other
+ * kernels, such as the agent model's, are running.  It allocates nothing: the
+ * step's scratch (per-tile partial sums, boundary values, TMA descriptors)
+ * lives in one fixed 4 MiB device array inside this library, present on every
+ * GPU that loads it until the process exits; b->workspace is ignored.
+ *  - prepare != 0 (re)initialises that scratch for this batch (as
+ *    hb_fused_prepare does for a workspace), then runs nsteps steps; pass it
+ *    on the first call and whenever the batch or its control blocks change.
+ *  - Limits: hb_fused_workspace_size(b) <= 4 MiB (about 120,000 tiles, e.g.
+ *    120 M cells with 32 x 32 tiles) and at most 256 instances; larger
+ *    batches get HB_ERR_LIMIT with a message.
+ *  - The first call on a device looks up the array's device address; make
+ *    that first call before any stream capture.
+ *  - Every call on a device shares the one array and leaves its contents
+ *    behind: calls that overlap on the GPU (other streams, other threads)
+ *    race with each other. */
+int hb_fused_step_noalloc(const struct hb_fused_batch *batch, int nsteps, int prepare,
+                          void *stream);
+
 /* ======================================================================
  * Coupling gather (no reference counterpart; replaces the
  * h[idx_target_ABM1] gather of CHANS-HiPIMS/CHANS-HiPIMS_server.py:255-256).
