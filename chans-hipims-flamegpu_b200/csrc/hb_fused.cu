@@ -28,6 +28,7 @@
 #include <stdint.h>
 
 #include <cuda.h>
+#include <cuda/atomic>
 
 #include <mutex>
 #include <vector>
@@ -302,6 +303,8 @@ __device__ void finalize_instance(const hb_instance &in, int ii, TilePartial *pa
     red_i[wid] = dry;
   }
   __syncthreads();
+  __shared__ double s_tnew;
+  __shared__ int s_halt;
   if (tid == 0) {
     double V = 0, O = 0, SM = 0;
     int D = 0;
@@ -338,12 +341,41 @@ __device__ void finalize_instance(const hb_instance &in, int ii, TilePartial *pa
     ctrl->cur = 1 - ctrl->cur;
     ctrl->step += 1;
     if (tnew >= ctrl->t_end) ctrl->halted = 1;
-    ctrl->rain_rate = rain_rate_at(in, ctrl, tnew);
-    bc_values_exact(in, tnew, &bct[ii]);
-    bc_values_at(in, ctrl, tnew);
-    __threadfence();
-    ctrl->tiles_done = 0u;
+    s_tnew = tnew;
   }
+  __syncthreads();
+  const double tnew = s_tnew;
+  // boundary values of the next step, one class per thread (step-function
+  // lookup, HC/flucCal_2ndOrder_jh_improved_Kernel.cu:355-366, 441-446)
+  if (tid < HB_MAX_CLASSES) {
+    const int k = tid, id = in.bc_id[k];
+    double hb = 0, wlb = 0, qxb = 0, qyb = 0;
+    if (in.given_depth && id + 1 < in.depth_cols) {
+      const int tl = timelevel(tnew, in.given_depth, in.depth_rows, in.depth_cols);
+      hb = in.given_depth[(int64_t)tl * in.depth_cols + id + 1];
+    }
+    if (in.given_wl && id + 1 < in.wl_cols) {
+      const int tl = timelevel(tnew, in.given_wl, in.wl_rows, in.wl_cols);
+      wlb = in.given_wl[(int64_t)tl * in.wl_cols + id + 1];
+    }
+    if (in.given_q && 2 + 2 * id < in.q_cols) {
+      const int tl = timelevel(tnew, in.given_q, in.q_rows, in.q_cols);
+      qxb = in.given_q[(int64_t)tl * in.q_cols + 1 + 2 * id];
+      qyb = in.given_q[(int64_t)tl * in.q_cols + 2 + 2 * id];
+    }
+    bct[ii].v[k][0] = hb;
+    bct[ii].v[k][1] = wlb;
+    bct[ii].v[k][2] = qxb;
+    bct[ii].v[k][3] = qyb;
+    ctrl->bc_vals[k][0] = (float)hb;
+    ctrl->bc_vals[k][1] = (float)wlb;
+    ctrl->bc_vals[k][2] = (float)qxb;
+    ctrl->bc_vals[k][3] = (float)qyb;
+  } else if (tid == 32) {
+    ctrl->rain_rate = rain_rate_at(in, ctrl, tnew);
+  }
+  if (tid == 0) ctrl->tiles_done = 0u;
+  (void)s_halt;
 }
 
 // Workspace layout: [n_tiles] TilePartial, [n_instances] BcTable, then
@@ -672,9 +704,10 @@ fused_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restri
         p.any_dry |= s.red_i[w];
       }
       partials[tile] = p;
-      __threadfence();
       const unsigned n_inst_tiles = (unsigned)(in.tiles_x * in.tiles_y);
-      s.last = (atomicAdd(&ctrl->tiles_done, 1u) == n_inst_tiles - 1);
+      // release: this tile's partial is visible before the count moves
+      cuda::atomic_ref<unsigned, cuda::thread_scope_device> done(ctrl->tiles_done);
+      s.last = (done.fetch_add(1u, cuda::memory_order_acq_rel) == n_inst_tiles - 1);
     }
     __syncthreads();
 
@@ -717,8 +750,8 @@ struct RowsSmem {
   T hmax[TY * kTW];           // h_max of the tile's cells
   uint8_t code[SH * kSWC];
   alignas(8) unsigned long long bar;
-  T xe[kRowsNW][R][4];        // face between cols 31 | 32: fh, fx, fy, sa
-  T sxw[kRowsNW][R][4];       // x-slope of col -1: h, z, qx, qy
+  T xe[TY][4];                // face between cols 31 | 32: fh, fx, fy, sa
+  T sxw[TY][4];               // x-slope of col -1: h, z, qx, qy
   double bc[HB_MAX_CLASSES][4];
   int bctype[HB_MAX_CLASSES];
   T manning[HB_MAX_ZONES];
@@ -1047,27 +1080,32 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
     __syncthreads();
 
     const int r0 = w * R;
-    // --- per warp: x-slope of column -1 and the face between columns 31|32
-    if (lane < R) {
-      const int i = r0 + lane;
-      const Cell<T> cm2 = V.cell(i, -2), cm1 = V.cell(i, -1), c0 = V.cell(i, 0);
-      const Slope<T> sm1 = slope_of(cm1, cm2, is_valid(V.code(i, -2)), c0,
-                                    is_valid(V.code(i, 0)));
-      s.sxw[w][lane][0] = sm1.h;
-      s.sxw[w][lane][1] = sm1.z;
-      s.sxw[w][lane][2] = sm1.qx;
-      s.sxw[w][lane][3] = sm1.qy;
-      const Cell<T> a = V.cell(i, 31), b = V.cell(i, 32);
-      const uint8_t ca = V.code(i, 31), cb = V.code(i, 32);
-      const Slope<T> sa = slope_of(a, V.cell(i, 30), is_valid(V.code(i, 30)), b, is_valid(cb));
-      const Slope<T> sb = slope_of(b, a, is_valid(ca), V.cell(i, 33), is_valid(V.code(i, 33)));
-      const FaceOut<T> f = face_any<T, FAST, 0>(s, a, ca, b, cb, sa, sb, datum_tile);
-      s.xe[w][lane][0] = f.fh;
-      s.xe[w][lane][1] = f.fx;
-      s.xe[w][lane][2] = f.fy;
-      s.xe[w][lane][3] = f.sa;
+    // --- tile edges, all lanes busy: warp 0 evaluates the faces between
+    // columns 31 | 32 (the east faces of lane 31), warp 1 the x-slopes of
+    // column -1 (needed by lane 0's west faces), for every row of the tile
+    if (w == 0) {
+      for (int i = lane; i < TY; i += 32) {
+        const Cell<T> a = V.cell(i, 31), b = V.cell(i, 32);
+        const uint8_t ca = V.code(i, 31), cb = V.code(i, 32);
+        const Slope<T> sa = slope_of(a, V.cell(i, 30), is_valid(V.code(i, 30)), b, is_valid(cb));
+        const Slope<T> sb = slope_of(b, a, is_valid(ca), V.cell(i, 33), is_valid(V.code(i, 33)));
+        const FaceOut<T> f = face_any<T, FAST, 0>(s, a, ca, b, cb, sa, sb, datum_tile);
+        s.xe[i][0] = f.fh;
+        s.xe[i][1] = f.fx;
+        s.xe[i][2] = f.fy;
+        s.xe[i][3] = f.sa;
+      }
+    } else if (w == 1) {
+      for (int i = lane; i < TY; i += 32) {
+        const Cell<T> cm2 = V.cell(i, -2), cm1 = V.cell(i, -1), c0 = V.cell(i, 0);
+        const Slope<T> sm1 = slope_of(cm1, cm2, is_valid(V.code(i, -2)), c0,
+                                      is_valid(V.code(i, 0)));
+        s.sxw[i][0] = sm1.h;
+        s.sxw[i][1] = sm1.z;
+        s.sxw[i][2] = sm1.qx;
+        s.sxw[i][3] = sm1.qy;
+      }
     }
-    __syncwarp();
 
     // --- column window: rows r0-2 .. r0+2
     const int j = lane;
@@ -1087,6 +1125,7 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
       // face between rows r0-1 (north) and r0 (south), from the south side
       nf = face_any<T, FAST, 1>(s, cC, kC, cN, kN, syC, syN, datum_tile);
     }
+    __syncthreads();  // tile-edge faces and slopes ready
     // per-thread partial sums over this warp's rows (<= 16 cells) in T; the
     // tile and instance reductions are FP64
     T vol_t = T(0), smax_t = T(0);
@@ -1110,10 +1149,10 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
       sxW.qx = __shfl_up_sync(0xffffffffu, sxC.qx, 1);
       sxW.qy = __shfl_up_sync(0xffffffffu, sxC.qy, 1);
       if (lane == 0) {
-        sxW.h = s.sxw[w][i - r0][0];
-        sxW.z = s.sxw[w][i - r0][1];
-        sxW.qx = s.sxw[w][i - r0][2];
-        sxW.qy = s.sxw[w][i - r0][3];
+        sxW.h = s.sxw[i][0];
+        sxW.z = s.sxw[i][1];
+        sxW.qx = s.sxw[i][2];
+        sxW.qy = s.sxw[i][3];
       }
       // west face (this cell is B) -> the west neighbour's east face
       const FaceOut<T> wf = face_any<T, FAST, 0>(s, cW, kW, cC, kC, sxW, sxC, datum_tile);
@@ -1122,10 +1161,10 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
       T ef_y = __shfl_down_sync(0xffffffffu, wf.fy, 1);
       T ef_a = __shfl_down_sync(0xffffffffu, wf.sa, 1);
       if (lane == 31) {
-        ef_h = s.xe[w][i - r0][0];
-        ef_x = s.xe[w][i - r0][1];
-        ef_y = s.xe[w][i - r0][2];
-        ef_a = s.xe[w][i - r0][3];
+        ef_h = s.xe[i][0];
+        ef_x = s.xe[i][1];
+        ef_y = s.xe[i][2];
+        ef_a = s.xe[i][3];
       }
       // south face (this cell is B, the row below is A)
       const FaceOut<T> sf = face_any<T, FAST, 1>(s, cS, kS, cC, kC, syS, syC, datum_tile);
@@ -1295,9 +1334,10 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
         p.any_dry |= s.red_i[q];
       }
       partials[tile] = p;
-      __threadfence();
       const unsigned n_inst_tiles = (unsigned)(in.tiles_x * in.tiles_y);
-      s.last = (atomicAdd(&ctrl->tiles_done, 1u) == n_inst_tiles - 1);
+      // release: this tile's partial is visible before the count moves
+      cuda::atomic_ref<unsigned, cuda::thread_scope_device> done(ctrl->tiles_done);
+      s.last = (done.fetch_add(1u, cuda::memory_order_acq_rel) == n_inst_tiles - 1);
     }
     __syncthreads();
     if (s.last) finalize_instance<T, kRowsNT>(in, ii, partials, bct, s.red_d, s.red_s, s.red_i);
