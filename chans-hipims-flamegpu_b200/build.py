@@ -33,7 +33,7 @@ PER_FILE = {
     "hb_compat.cu": ["-fmad=false"],
     "hb_fused.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
 }
-SOURCES = ["hb_abi.cpp", "hb_compat.cu", "hb_fused.cu"]
+SOURCES = ["hb_abi.cpp", "hb_compat.cu", "hb_fused.cu", "hb_adjoint.cu"]
 
 
 def nvcc() -> str:

@@ -76,6 +76,20 @@ class HbFusedBatch(ctypes.Structure):
 
 # name -> (restype, argtypes)
 _I, _P, _L = c_i32, c_vp, c_i64
+class HbAdjointArgs(ctypes.Structure):
+    """Mirror of hb_adjoint_args (include/hipims_b200.h)."""
+    _fields_ = [
+        ("instance", c_vp), ("rows", c_i32), ("cols", c_i32), ("pitch", c_i32),
+        ("code_pitch", c_i32),
+        ("h", c_vp), ("qx", c_vp), ("qy", c_vp),
+        ("lam_h", c_vp), ("lam_qx", c_vp), ("lam_qy", c_vp),
+        ("out_h", c_vp), ("out_qx", c_vp), ("out_qy", c_vp),
+        ("mu", c_vp), ("mu_stride", c_i64), ("grad", c_vp),
+        ("t", c_dbl), ("dt", c_dbl), ("rain_rate", c_dbl), ("rain_base", c_dbl),
+        ("first", c_i32), ("pad", c_i32),
+    ]
+
+
 SIGNATURES = {
     "hb_abi_version": (_I, []),
     "hb_last_error": (ctypes.c_char_p, []),
@@ -95,6 +109,8 @@ SIGNATURES = {
     "hb_fused_prepare": (_I, [_P, _P]),
     "hb_fused_step": (_I, [_P, _I, _P]),
     "hb_fused_step_noalloc": (_I, [_P, _I, _I, _P]),
+    "hb_adjoint_step": (_I, [_P, _P]),
+    "hb_adjoint_gauge": (_I, [_L, _P, _P, _P, _P, ctypes.c_double, _P]),
     "hb_gather": (_I, [_I, _L, _P, _P, _P, _P, _P, _P, _P, _P]),
 }
 

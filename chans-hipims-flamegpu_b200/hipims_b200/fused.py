@@ -121,11 +121,13 @@ class _Instance:
         h = dense(c.h)
         qx = dense(c.qx)
         qy = dense(c.qy)
+        self.initial = (h.clone(), qx.clone(), qy.clone())
         self.h = [h, h.clone()]
         self.qx = [qx, qx.clone()]
         self.qy = [qy, qy.clone()]
         self.z = dense(zrel)
         self.h_max = dense(c.h if c.h_max is None else c.h_max)
+        self.initial_h_max = self.h_max.clone()
         self.code = torch.as_tensor(code_np, device=device).contiguous()
         self.datum = torch.as_tensor(datum, dtype=torch.float32, device=device).contiguous()
         self.z_abs_offset = dfull
@@ -231,6 +233,7 @@ class FusedSolver:
             tile_inst.extend([k] * nt)
             begin += nt
         self.n_tiles = begin
+        self._ctrl_init = bytes(ctrl_host)
         self.ctrl.copy_(torch.frombuffer(bytearray(ctrl_host), dtype=torch.uint8))
         self._recs_host = recs
         self.records = torch.frombuffer(bytearray(recs), dtype=torch.uint8).to(self.device)
@@ -256,6 +259,39 @@ class FusedSolver:
         self.prepare()
 
     # ----------------------------------------------------------------- control
+    def record_ptr(self, k: int = 0) -> int:
+        """Device address of instance k's hb_instance record."""
+        return self.records.data_ptr() + k * ctypes.sizeof(_lib.HbInstance)
+
+    def set_manning(self, k: int, manning: Sequence[float]) -> None:
+        """Replace the Manning coefficients (per zone) of instance k."""
+        if len(manning) > _lib.HB_MAX_ZONES:
+            raise ValueError(f"at most {_lib.HB_MAX_ZONES} Manning zones")
+        vals = [float(v) for v in manning] + [0.0] * (_lib.HB_MAX_ZONES - len(manning))
+        self.inst[k].manning = vals
+        for z_ in range(_lib.HB_MAX_ZONES):
+            self._recs_host[k].manning[z_] = vals[z_]
+        self.records.copy_(torch.frombuffer(bytearray(self._recs_host), dtype=torch.uint8))
+
+    def reset(self, rain_mult: Sequence[float] | float | None = None) -> None:
+        """Back to the initial state and control blocks of the catchments
+        (t0, dt0, step 0), optionally with new rain multipliers; re-prepares."""
+        n = len(self.inst)
+        arr = (_lib.HbCtrl * n).from_buffer_copy(self._ctrl_init)
+        if rain_mult is not None:
+            mult = [rain_mult] * n if np.isscalar(rain_mult) else list(rain_mult)
+            for k in range(n):
+                arr[k].rain_mult = float(mult[k])
+        for ins in self.inst:
+            h0, qx0, qy0 = ins.initial
+            for buf in range(2):
+                ins.h[buf].copy_(h0)
+                ins.qx[buf].copy_(qx0)
+                ins.qy[buf].copy_(qy0)
+            ins.h_max.copy_(ins.initial_h_max)
+        self.ctrl.copy_(torch.frombuffer(bytearray(arr), dtype=torch.uint8))
+        self.prepare()
+
     def _stream(self) -> int:
         return torch.cuda.current_stream(self.device).cuda_stream
 

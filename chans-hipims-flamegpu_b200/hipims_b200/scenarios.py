@@ -12,6 +12,10 @@ the shapes, sizes and value ranges of the workload it stands for.
                    dry start; uniform rain 50 mm/h for 3600 s
   ensemble         catchments with sides drawn from 256-1536 cells, each with
                    its own double-triangle hyetograph (peaks 20-120 mm/h)
+  adjoint_case     n x n (1024 in the headline case) DEM as urban_catchment,
+                   16 Voronoi Manning zones from seeded sites with n drawn
+                   from U(0.02, 0.10), 32 gauges on random valid cells,
+                   rain 50 mm/h, optional initial pond
   channel          the 25 x 225 back-channel case: H_GIVEN inflow, OPEN
                    outflow, walls (HP/backCase.ipynb scenario, own geometry)
 
@@ -161,3 +165,41 @@ def channel(n_rows: int = 25, n_cols: int = 225, dx: float = 0.2012, inflow_h: f
                 given_depth=np.array([[0.0, inflow_h], [600.0, inflow_h]]),
                 given_q=np.array([[0.0, 0.202, 0.0], [600.0, 0.202, 0.0]]),
                 rain=np.array([[0.0, 0.0], [200.0, 0.0]]), t_end=8.0)
+
+
+def voronoi_zones(n_rows: int, n_cols: int, n_zones: int, seed: int) -> np.ndarray:
+    """Zone of every cell: index of the nearest of n_zones seeded sites."""
+    rng = np.random.default_rng(seed)
+    sites = rng.uniform(0.0, 1.0, (n_zones, 2)) * np.array([n_rows, n_cols])
+    zone = np.empty((n_rows, n_cols), dtype=np.uint8)
+    cc = np.arange(n_cols, dtype=np.float64)
+    for r in range(n_rows):
+        d = (r - sites[:, 0:1]) ** 2 + (cc[None, :] - sites[:, 1:2]) ** 2
+        zone[r] = np.argmin(d, axis=0)
+    return zone
+
+
+def adjoint_case(n: int = 1024, dx: float = 2.0, seed: int = 0, n_zones: int = 16,
+                 n_gauges: int = 32, rain_mm_h: float = 50.0, pond: float = 0.0,
+                 relief: float = 50.0) -> dict:
+    """Manning-calibration case: DEM as urban_catchment, Voronoi zones with
+    true n ~ U(0.02, 0.10), gauges on random valid cells.  pond > 0 adds an
+    initial water level pond m above the lowest quarter of the bed."""
+    d = urban_catchment(n, dx=dx, seed=seed, rain_mm_h=rain_mm_h)
+    if relief != 50.0:
+        zi, _ = urban_dem(n, n, seed, relief=relief)
+        d["z"][1:-1, 1:-1] = zi
+    rng = np.random.default_rng(seed + 104729)
+    zone = np.zeros(d["mask"].shape, dtype=np.uint8)
+    zone[1:-1, 1:-1] = voronoi_zones(n, n, n_zones, seed + 31)
+    d["landuse"] = zone
+    d["manning"] = list(rng.uniform(0.02, 0.10, n_zones))
+    valid = d["mask"] > 0
+    if pond > 0.0:
+        zin = d["z"][valid]
+        level = np.quantile(zin, 0.25) + pond
+        d["h"] = np.where(valid, np.maximum(level - d["z"], 0.0), 0.0)
+    rr, cc = np.nonzero(valid)
+    pick = rng.choice(rr.size, size=n_gauges, replace=False)
+    d["gauge_rows"], d["gauge_cols"] = rr[pick], cc[pick]
+    return d

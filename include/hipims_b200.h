@@ -155,6 +155,35 @@ int hb_fused_step_noalloc(const struct hb_fused_batch *batch, int nsteps, int pr
                           void *stream);
 
 /* ======================================================================
+ * Discrete adjoint of the FP64 fused step (no reference counterpart).
+ * Given lambda^{n+1} = dJ/dU^{n+1} (U = h, qx, qy on the dense layout of
+ * one instance) and the forward state U^n, writes lambda^n = (dU^{n+1}/dU^n)^T
+ * lambda^{n+1} and adds (dU^{n+1}/dtheta)^T lambda^{n+1} to grad, theta =
+ * (Manning n of zones 0..15, rain multiplier).  dt is frozen (the forward's
+ * schedule); every discrete decision is the forward's.
+ * ==================================================================== */
+typedef struct hb_adjoint_args {
+  const struct hb_instance *instance; /* device record of the instance (FP64) */
+  int32_t rows, cols, pitch, code_pitch;
+  const double *h, *qx, *qy;          /* U^n, dense */
+  const double *lam_h, *lam_qx, *lam_qy; /* lambda^{n+1} */
+  double *out_h, *out_qx, *out_qy;    /* lambda^n (overwritten) */
+  double *mu;                         /* scratch: 3 * mu_stride doubles */
+  int64_t mu_stride;                  /* >= elements of one dense array */
+  double *grad;                       /* [17]: d/dn_zone (16), d/d rain multiplier */
+  double t, dt;                       /* time and time step of step n */
+  double rain_rate;                   /* rain rate used by step n (m/s) */
+  double rain_base;                   /* the same without the multiplier */
+  int32_t first;                      /* step n starts at t == 0 */
+  int32_t pad;
+} hb_adjoint_args;
+int hb_adjoint_step(const hb_adjoint_args *args, void *stream);
+/* lam_h[offsets[i]] += 2 * weight * (h[offsets[i]] - obs[i]): the gradient of
+ * a sum of squared gauge misfits, added at a sampled step. */
+int hb_adjoint_gauge(int64_t n, const int64_t *offsets, const double *h, const double *obs,
+                     double *lam_h, double weight, void *stream);
+
+/* ======================================================================
  * Coupling gather (no reference counterpart; replaces the
  * h[idx_target_ABM1] gather of CHANS-HiPIMS/CHANS-HiPIMS_server.py:255-256).
  * Gathers depth (and optionally velocities u = qx/h, v = qy/h, 0 when dry)

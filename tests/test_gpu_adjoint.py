@@ -1,0 +1,149 @@
+"""Discrete adjoint (hb_adjoint_step / hb_adjoint_gauge through
+hipims_b200.adjoint) against central finite differences of the frozen-dt FP64
+forward.
+
+The finite-difference checks run on rough, everywhere-wet states (white-noise
+bed, depths and discharges) that stay wet over the checked horizon.  Three
+properties of the reference scheme decide that choice:
+  * its friction update (HC/friction_implicit_andUpdate_jh_Kernel.cu:61-133)
+    forms 1 - sqrt(1 + 4x) with x = dt g n^2 h^(-7/3) |q|, which loses
+    log10(1/x) digits; in deep, slow water (x ~ 1e-6) the Manning term of the
+    FP64 forward carries ~1e-4 relative rounding noise, so a difference
+    quotient in n cannot be resolved there;
+  * minmod slope limiting is a kink wherever two neighbouring differences
+    tie, which smooth fields do at almost every face, so differences of
+    smooth states straddle kinks at any practical step;
+  * the wet/dry threshold (h_small), the flux mask and the Froude limiter make
+    the step discontinuous; across thin films the map is not differentiable
+    at any resolvable scale, and the adjoint (the derivative of the branch the
+    forward took) is checked there for finiteness only.
+"""
+import dataclasses
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from hipims_b200 import scenarios as S
+from hipims_b200.adjoint import GaugeMisfit, gauge_misfit, record_schedule
+
+pytestmark = pytest.mark.gpu
+
+NSTEPS, EVERY, K = 120, 10, 50
+# Central differences: parameters with a relative step of 1e-5, initial state
+# with an absolute step of 1e-7 (m or m^2/s) along a random direction.
+EPS_PARAM = 1e-5
+EPS_STATE = 1e-7
+# Agreement, relative to the largest gradient component.
+GRAD_RTOL = 1e-4
+
+
+def rough_wet(n=48, seed=3, n_zones=4, n_gauges=12):
+    """White-noise bed (0-0.2 m), depth (0.4-0.5 m) and discharges on an open
+    square: stays wet (h > 0.1 m) for the first 120 steps."""
+    d = S.adjoint_case(n, relief=0.5, n_zones=n_zones, n_gauges=n_gauges, seed=seed)
+    valid = d["mask"] > 0
+    r = np.random.default_rng(seed + 99)
+    sh = valid.shape
+    d["z"] = np.where(valid, 0.2 * r.uniform(0, 1, sh), 0.0)
+    d["h"] = np.where(valid, 0.4 + 0.1 * r.uniform(0, 1, sh), 0.0)
+    d["qx"] = np.where(valid, 0.1 + 0.05 * r.standard_normal(sh), 0.0)
+    d["qy"] = np.where(valid, -0.05 + 0.05 * r.standard_normal(sh), 0.0)
+    d["first_dt"] = 0.1
+    return d
+
+
+@pytest.fixture(scope="module")
+def case(cuda):
+    d = rough_wet()
+    c = S.catchment_from(d, t_end=math.inf)
+    dts = record_schedule(c, NSTEPS, device=cuda)
+    truth = GaugeMisfit(c, d["gauge_rows"], d["gauge_cols"], NSTEPS, dts, EVERY, K,
+                        device=cuda)
+    obs = truth.simulate(d["manning"], 1.0).clone()
+    p = GaugeMisfit(c, d["gauge_rows"], d["gauge_cols"], NSTEPS, dts, EVERY, K, obs=obs,
+                    device=cuda)
+    start = [v * 1.25 for v in d["manning"]]
+    return d, c, dts, p, start
+
+
+def _J(p, manning, mult):
+    return float(p.loss(p.simulate(manning, mult)))
+
+
+def test_parameter_gradient_matches_central_differences(case):
+    d, c, dts, p, start = case
+    p.simulate(start, 0.8)
+    g = p.gradient()
+    assert g.shape == (5,)
+    assert np.all(np.isfinite(g)) and np.abs(g).max() > 0
+    fd = []
+    for z in range(4):
+        e = EPS_PARAM * start[z]
+        up, dn = list(start), list(start)
+        up[z] += e
+        dn[z] -= e
+        fd.append((_J(p, up, 0.8) - _J(p, dn, 0.8)) / (2 * e))
+    e = EPS_PARAM * 0.8
+    fd.append((_J(p, start, 0.8 + e) - _J(p, start, 0.8 - e)) / (2 * e))
+    fd = np.array(fd)
+    assert np.abs(g - fd).max() <= GRAD_RTOL * np.abs(fd).max(), (g, fd)
+
+
+@pytest.mark.parametrize("which", ["h", "qx", "qy"])
+def test_state_gradient_dot_product(case, cuda, which):
+    """<dJ/dU0, v> against (J(U0 + eps v) - J(U0 - eps v)) / 2 eps."""
+    d, c, dts, p, start = case
+    p.simulate(start, 1.0)
+    _, lam0 = p.gradient(with_state=True)
+    valid = np.asarray(c.mask) > 0
+    v = np.where(valid, np.random.default_rng(5).standard_normal(valid.shape), 0.0)
+    adj = float((lam0[which].cpu().numpy() * v).sum())
+    base = np.asarray(getattr(c, which))
+    Js = []
+    for sgn in (1, -1):
+        cp = dataclasses.replace(c, **{which: base + sgn * EPS_STATE * v})
+        q = GaugeMisfit(cp, d["gauge_rows"], d["gauge_cols"], NSTEPS, dts, EVERY, K,
+                        obs=p.obs, device=cuda)
+        Js.append(_J(q, start, 1.0))
+    fd = (Js[0] - Js[1]) / (2 * EPS_STATE)
+    assert adj == pytest.approx(fd, rel=GRAD_RTOL)
+
+
+def test_autograd_function(case):
+    d, c, dts, p, start = case
+    n = torch.tensor(start, dtype=torch.float64, requires_grad=True)
+    r = torch.tensor(0.8, dtype=torch.float64, requires_grad=True)
+    J = gauge_misfit(p, n, r)
+    J.backward()
+    g = p.gradient()
+    assert float(J.detach()) == pytest.approx(_J(p, start, 0.8), rel=1e-12)
+    np.testing.assert_allclose(n.grad.numpy(), g[:4], rtol=1e-12)
+    assert float(r.grad) == pytest.approx(g[4], rel=1e-12)
+
+
+def test_checkpoint_interval_does_not_change_gradient(case, cuda):
+    d, c, dts, p, start = case
+    p.simulate(start, 0.8)
+    g1 = p.gradient()
+    q = GaugeMisfit(c, d["gauge_rows"], d["gauge_cols"], NSTEPS, dts, EVERY, 7, obs=p.obs,
+                    device=cuda)
+    q.simulate(start, 0.8)
+    g2 = q.gradient()
+    np.testing.assert_allclose(g2, g1, rtol=1e-12, atol=1e-300)
+
+
+def test_wet_dry_case_runs(cuda):
+    """Dry start with rain and an initial pond (the calibration case's shape):
+    finite gradients, and the loss at the true parameters is zero."""
+    d = S.adjoint_case(48, pond=0.5, relief=5.0, n_zones=4, n_gauges=8, seed=4)
+    c = S.catchment_from(d, t_end=math.inf)
+    dts = record_schedule(c, 60, device=cuda)
+    p = GaugeMisfit(c, d["gauge_rows"], d["gauge_cols"], 60, dts, 10, 25, device=cuda)
+    obs = p.simulate(d["manning"], 1.0).clone()
+    q = GaugeMisfit(c, d["gauge_rows"], d["gauge_cols"], 60, dts, 10, 25, obs=obs, device=cuda)
+    assert _J(q, d["manning"], 1.0) == 0.0
+    q.simulate([v * 1.3 for v in d["manning"]], 1.1)
+    g = q.gradient()
+    assert np.all(np.isfinite(g)) and np.abs(g).max() > 0
