@@ -11,7 +11,9 @@ fused launch advancing every valid cell (4,194,304) by one time step.
 Timing: 8 untimed spin-up steps (the dry start becomes wet everywhere), W
 untimed warm-up steps, then K timed steps.  Each timed step is bracketed by
 CUDA events on the launching stream; a 256 MiB buffer is written between timed
-steps to flush the 126 MB L2.  N > 1 (torchrun): every rank advances its own
+steps to flush the 126 MB L2.  nvidia-smi samples the SM clock every 200 ms
+from before the first timed step to after the last (the default K keeps the
+timed region above one second so that it holds several samples).  N > 1 (torchrun): every rank advances its own
 replica (weak scaling; the catchment does not shard without a halo exchange),
 the time is the max over ranks and `value` counts the cells of all ranks.
 
@@ -65,6 +67,18 @@ def config_of(n: int, world: int, extra: dict | None = None) -> dict:
 
 class Clocks:
     """nvidia-smi sampler for the timed region."""
+
+    def wait_first_sample(self, timeout: float = 5.0) -> None:
+        """Block until the sampler has written its first line (nvidia-smi
+        takes a few hundred ms to start)."""
+        t0 = time.time()
+        while self.proc is not None and time.time() - t0 < timeout:
+            try:
+                if os.path.getsize(self.path) > 0:
+                    return
+            except OSError:
+                pass
+            time.sleep(0.05)
 
     def __init__(self, gpu: int):
         self.path = tempfile.mktemp(suffix=".csv")
@@ -173,7 +187,8 @@ def run_ours(args) -> None:
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     d = workload(args.cells)
-    fs = FusedSolver(catchment_from(d), dtype=torch.float32, tile=tuple(args.tile), device=dev)
+    fs = FusedSolver(catchment_from(d), dtype=torch.float32, tile=tuple(args.tile), device=dev,
+                     minb=args.minb)
     n_valid = fs.inst[0].n_valid
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -187,6 +202,7 @@ def run_ours(args) -> None:
         torch.cuda.synchronize(dev)
 
     clocks = Clocks(local)
+    clocks.wait_first_sample()
     barrier()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
@@ -215,10 +231,11 @@ def run_ours(args) -> None:
     for hsrc, x in zip(host_in, (ins.h[c.cur], ins.qx[c.cur], ins.qy[c.cur])):
         hsrc.copy_(x)
     cur = c.cur
+    e2e_steps = min(args.steps, 200)
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(e2e_steps):
         for hsrc, x in zip(host_in, (ins.h[cur], ins.qx[cur], ins.qy[cur])):
             x.copy_(hsrc, non_blocking=True)
         fs.step(1)
@@ -232,7 +249,7 @@ def run_ours(args) -> None:
         t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    e2e = world * n_valid * args.steps / (e2e_ms * 1e-3) / 1e9
+    e2e = world * n_valid * e2e_steps / (e2e_ms * 1e-3) / 1e9
     bytes_io = sum(x.numel() * x.element_size() for x in host_in)
 
     if rank == 0:
@@ -246,20 +263,23 @@ def run_ours(args) -> None:
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "impl": "ours",
             "config": config_of(args.cells, world, {"tile": list(args.tile),
+                                                     "min_blocks_per_sm": args.minb,
                                                      "sim_time_s": c.t, "dt_s": c.dt}),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
-                         "kernel": f"rows_step_kernel<float,{args.tile[0]}>",
+                         "kernel": f"rows_step_kernel<float,{args.tile[0]},minb={args.minb}>",
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "traffic": profiled_traffic()},
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": bytes_io,
-                    "d2h_bytes_per_step": bytes_io},
+                    "d2h_bytes_per_step": bytes_io, "steps": e2e_steps,
+                    "path": "pinned host h, qx, qy -> device; hb_fused_step; device -> "
+                            "pinned host, every step"},
             "gpu_launches": args.steps,
             "clocks": clk,
             "step_ms_min": min(step_ms), "step_ms_max": max(step_ms),
         }
         if args.accuracy:
-            line["accuracy"] = accuracy_vs_fp64(d, dev, SPINUP + args.warmup + args.steps)
+            line["accuracy"] = accuracy_vs_fp64(d, dev)
         if args.plain and world == 1:
             pl = plain_fp64_rate(d, dev)
             pl["fused_fp32_over_plain"] = value / pl["value"]
@@ -269,6 +289,8 @@ def run_ours(args) -> None:
             if "fp64_plain" in line:
                 en["over_plain_fp64"] = en["value"] / line["fp64_plain"]["value"]
             line["ensemble"] = en
+        if args.adjoint and world == 1:
+            line["adjoint"] = adjoint_cost(dev, args.adjoint_cells, args.adjoint_steps)
         if args.cpu_baseline and world == 1:
             line["cpu_baseline"] = {k: v for k, v in cpu_reference_rate(
                 d, args.cpu_steps, 0).items() if k in ("value", "unit", "cores", "kind",
@@ -344,47 +366,136 @@ def ensemble_rate(dev, steps: int, count: int = 64, seed: int = 0) -> dict:
             "tile": list(cfg["tile"]), "minb": cfg.get("minb", 0)}
 
 
-def accuracy_vs_fp64(d: dict, dev, steps: int) -> dict:
+def adjoint_cost(dev, n: int = 1024, steps: int = 2000, K: int = 100, every: int = 10,
+                 fd: bool = True) -> dict:
+    """Config 4: Manning calibration on an n x n catchment with 16 Voronoi
+    zones and 32 gauges sampled every 10 steps; cost of the checkpointed
+    adjoint (recompute included) against the forward, and the gradient against
+    central differences (relative step 1e-5) of the same frozen-dt forward."""
+    from hipims_b200 import scenarios as S
+    from hipims_b200.adjoint import GaugeMisfit, record_schedule
+    from hipims_b200.scenarios import catchment_from
+
+    d = S.adjoint_case(n, seed=0)
+    c = catchment_from(d)
+    dts = record_schedule(c, steps, device=dev)
+    truth = GaugeMisfit(c, d["gauge_rows"], d["gauge_cols"], steps, dts, every, K, device=dev)
+    obs = truth.simulate(d["manning"], 1.0).clone()
+    del truth
+    p = GaugeMisfit(c, d["gauge_rows"], d["gauge_cols"], steps, dts, every, K, obs=obs,
+                    device=dev)
+    start = [v * 1.25 for v in d["manning"]]
+    p.simulate(start, 0.8)
+    p.gradient()  # warm-up
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    p.simulate(start, 0.8)
+    torch.cuda.synchronize(dev)
+    t_fwd = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    g = p.gradient()
+    torch.cuda.synchronize(dev)
+    t_adj = time.perf_counter() - t0
+    # the forward alone, without checkpoints or gauge samples
+    p.fs.reset(0.8)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    p.fs.step(steps)
+    torch.cuda.synchronize(dev)
+    t_plain = time.perf_counter() - t0
+    out = {"cells": int(p.fs.inst[0].n_valid), "steps": steps, "checkpoint": K,
+           "zones": len(d["manning"]), "gauges": int(p.n_gauges), "sample_every": every,
+           "forward_s": t_fwd, "forward_plain_s": t_plain, "adjoint_s": t_adj,
+           "adjoint_over_forward": t_adj / t_fwd, "dtype": "f64",
+           "grad_abs_max": float(np.abs(g).max())}
+    if fd:
+        J = lambda m, r: float(p.loss(p.simulate(m, r)))
+
+        def central(rel):
+            res = []
+            for z in range(len(start) + 1):
+                base = start[z] if z < len(start) else 0.8
+                e = rel * base
+                if z < len(start):
+                    up, dn = list(start), list(start)
+                    up[z] += e
+                    dn[z] -= e
+                    res.append((J(up, 0.8) - J(dn, 0.8)) / (2 * e))
+                else:
+                    res.append((J(start, 0.8 + e) - J(start, 0.8 - e)) / (2 * e))
+            return np.asarray(res)
+
+        f4, f5 = central(1e-4), central(1e-5)
+        scale = float(np.abs(f5).max())
+        stable = np.abs(f4 - f5) <= 1e-4 * scale
+        err = np.abs(g - f5) / scale
+        out["fd"] = {
+            "rel_steps": [1e-4, 1e-5], "params": len(g),
+            "resolvable": int(stable.sum()),
+            "resolvable_rule": "|fd(1e-4) - fd(1e-5)| <= 1e-4 max|fd|",
+            "max_err_over_max_grad_resolvable": float(err[stable].max()) if stable.any()
+            else None,
+            "max_err_over_max_grad_all": float(err.max()),
+            "adjoint": [float(x) for x in g], "fd_1e-5": [float(x) for x in f5],
+            "fd_1e-4": [float(x) for x in f4]}
+    return out
+
+
+def accuracy_vs_fp64(d: dict, dev, horizons=(64, 1000)) -> dict:
     """Max depth / velocity difference of the FP32 fused run against the FP64
     fused run at identical simulated times (the FP64 dt sequence replayed), and
-    the FP64 volume balance of the FP32 run."""
+    the FP64 volume balance of the FP32 run, after each horizon (steps from
+    the dry start)."""
     from hipims_b200.fused import FusedSolver
     from hipims_b200.scenarios import catchment_from
 
+    horizons = sorted(horizons)
     f64 = FusedSolver(catchment_from(d), dtype=torch.float64, device=dev)
-    dts = []
-    for _ in range(steps):
+    dts, ref = [], {}
+    for k in range(1, horizons[-1] + 1):
         f64.step(1)
         dts.append(f64.controls()[0].dt)
+        if k in horizons:
+            ref[k] = f64.compacted()
+    del f64
     f32 = FusedSolver(catchment_from(d, dt_replay=np.asarray(dts)), dtype=torch.float32,
                       device=dev)
-    f32.step(steps)
-    a, b = f32.compacted(), f64.compacted()
-    wet = b["h"] > 1e-3
-    ua = np.where(wet, a["qx"] / np.maximum(a["h"], 1e-3), 0)
-    ub = np.where(wet, b["qx"] / np.maximum(b["h"], 1e-3), 0)
-    c = f32.controls()[0]
-    bal = abs(c.volume - c.volume0 - c.rain_volume + c.outflow_volume) / max(c.rain_volume,
-                                                                               1e-30)
-    return {"steps": steps, "sim_time_s": c.t, "max_abs_dh_m": float(np.abs(a["h"] - b["h"]).max()),
-            "max_abs_du_ms_wet": float(np.abs(ua - ub).max()),
-            "volume_balance_rel_err": bal, "reference": "FP64 fused run, same dt sequence"}
+    out, done = [], 0
+    for k in horizons:
+        f32.step(k - done)
+        done = k
+        a, b = f32.compacted(), ref[k]
+        wet = b["h"] > 1e-3
+        ua = np.where(wet, a["qx"] / np.maximum(a["h"], 1e-3), 0)
+        ub = np.where(wet, b["qx"] / np.maximum(b["h"], 1e-3), 0)
+        c = f32.controls()[0]
+        bal = abs(c.volume - c.volume0 - c.rain_volume + c.outflow_volume) / max(
+            c.rain_volume, 1e-30)
+        out.append({"steps": k, "sim_time_s": c.t,
+                    "max_abs_dh_m": float(np.abs(a["h"] - b["h"]).max()),
+                    "max_abs_du_ms_wet": float(np.abs(ua - ub).max()),
+                    "volume_balance_rel_err": bal})
+    return {"horizons": out, "reference": "FP64 fused run, same dt sequence"}
 
 
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=5000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cells", type=int, default=N_CELLS)
-    ap.add_argument("--tile", type=int, nargs=2, default=[64, 32])
+    ap.add_argument("--tile", type=int, nargs=2, default=[32, 32])
+    ap.add_argument("--minb", type=int, default=5)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-accuracy", dest="accuracy", action="store_false")
     ap.add_argument("--no-plain", dest="plain", action="store_false")
     ap.add_argument("--no-ensemble", dest="ensemble", action="store_false")
     ap.add_argument("--ensemble-steps", type=int, default=20)
+    ap.add_argument("--no-adjoint", dest="adjoint", action="store_false")
+    ap.add_argument("--adjoint-cells", type=int, default=1024)
+    ap.add_argument("--adjoint-steps", type=int, default=2000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -21,7 +21,7 @@
 #include "hipims_b200.h"
 #include "hipims_b200_fused.h"
 
-static_assert(sizeof(hb_adjoint_args) == 160, "hb_adjoint_args layout (ctypes mirror)");
+static_assert(sizeof(hb_adjoint_args) == 168, "hb_adjoint_args layout (ctypes mirror)");
 
 namespace hb {
 namespace {
@@ -90,7 +90,8 @@ __device__ void load_bc(const hb_instance &in, double t, BcVals &bc) {
 // output adjoint `ob` and scatter into lam (atomics).
 template <int DIR>
 __device__ FaceOut5 face_at(const Grid &G, const BcVals &bc, int ra, int ca, int rb, int cb,
-                            const FaceOut5 *ob, double *lh, double *lqx, double *lqy) {
+                            const FaceOut5 *ob, double *lh, double *lqx, double *lqy,
+                            double hreg = 0.0) {
   const int dr = rb - ra, dc = cb - ca;  // unit step from A to B
   const bool va = G.valid(ra, ca), vb = G.valid(rb, cb);
   FaceOut5 o{0, 0, 0, 0, 0};
@@ -133,6 +134,7 @@ __device__ FaceOut5 face_at(const Grid &G, const BcVals &bc, int ra, int ca, int
   auto add = [&](int r, int c, const C3 &v) {
     if (!G.valid(r, c)) return;
     const size_t k = G.off(r, c);
+    if (G.h[k] < hreg) return;  // masked cell: its state adjoint stays zero
     if (v.h != 0.0) atomicAdd(lh + k, v.h);
     if (v.qx != 0.0) atomicAdd(lqx + k, v.qx);
     if (v.qy != 0.0) atomicAdd(lqy + k, v.qy);
@@ -207,9 +209,15 @@ adj_cell_kernel(hb_adjoint_args a) {
       C3 ub, rb;
       double nb;
       cell_rev(tp, ob, a.dt, ub, rb, nb);
-      a.out_h[k] = ub.h;
-      a.out_qx[k] = ub.qx;
-      a.out_qy[k] = ub.qy;
+      // Below h_reg the cell's state adjoint is held at zero.  The step never
+      // clamps h >= 0 (as the reference); negative depths and films of a few
+      // h_small on bumps between deeper cells, with discharges at rounding
+      // level, have linearised gains above one per step that the nonlinear
+      // step saturates, so the exact adjoint through them grows without bound.
+      const bool keep = !(u.h < a.h_reg);
+      a.out_h[k] = keep ? ub.h : 0.0;
+      a.out_qx[k] = keep ? ub.qx : 0.0;
+      a.out_qy[k] = keep ? ub.qy : 0.0;
       mu_h[k] = active ? rb.h : 0.0;
       mu_qx[k] = active ? rb.qx : 0.0;
       mu_qy[k] = active ? rb.qy : 0.0;
@@ -262,7 +270,7 @@ adj_face_kernel(hb_adjoint_args a) {
     const FaceOut5 ob{kk * (mB.h - mA.h), kk * (mB.qx - mA.qx), kk * (mB.qy - mA.qy),
                       -kk * mA.qx, kk * mB.qx};
     if (ob.fh != 0.0 || ob.fx != 0.0 || ob.fy != 0.0 || ob.sa != 0.0 || ob.sb != 0.0)
-      face_at<0>(G, bc, r, c - 1, r, c, &ob, a.out_h, a.out_qx, a.out_qy);
+      face_at<0>(G, bc, r, c - 1, r, c, &ob, a.out_h, a.out_qx, a.out_qy, a.h_reg);
   }
   // y-face between (r, c) = A (south) and (r - 1, c) = B (north)
   if (c < a.cols) {
@@ -270,7 +278,7 @@ adj_face_kernel(hb_adjoint_args a) {
     const FaceOut5 ob{kk * (mB.h - mA.h), kk * (mB.qx - mA.qx), kk * (mB.qy - mA.qy),
                       -kk * mA.qy, kk * mB.qy};
     if (ob.fh != 0.0 || ob.fx != 0.0 || ob.fy != 0.0 || ob.sa != 0.0 || ob.sb != 0.0)
-      face_at<1>(G, bc, r, c, r - 1, c, &ob, a.out_h, a.out_qx, a.out_qy);
+      face_at<1>(G, bc, r, c, r - 1, c, &ob, a.out_h, a.out_qx, a.out_qy, a.h_reg);
   }
 }
 

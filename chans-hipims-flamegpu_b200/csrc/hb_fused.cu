@@ -30,6 +30,7 @@
 #include <cuda.h>
 #include <cuda/atomic>
 
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -1345,16 +1346,36 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
   }
 }
 
-// Prepare: volume at t, rain rate and boundary values, counters.
+// Prepare: rain rate and boundary values at t, counters; the volume at t is
+// summed by prepare_volume_kernel, launched after this one.
 template <typename T>
 __global__ void __launch_bounds__(kNT)
 prepare_kernel(const hb_instance *__restrict__ insts, BcTable *__restrict__ bct) {
   const hb_instance &in = insts[blockIdx.x];
   hb_ctrl *c = in.ctrl;
+  if (threadIdx.x == 0) {
+    c->volume = 0.0;
+    c->volume0 = 0.0;
+    c->tiles_done = 0u;
+    c->rain_rate = rain_rate_at(in, c, c->t);
+    bc_values_exact(in, c->t, &bct[blockIdx.x]);
+    bc_values_at(in, c, c->t);
+  }
+}
+
+// Volume of every instance at t: blockIdx.y is the instance, the x blocks
+// share its cells; one FP64 atomic per block into volume and volume0.
+template <typename T>
+__global__ void __launch_bounds__(kNT)
+prepare_volume_kernel(const hb_instance *__restrict__ insts) {
+  const hb_instance &in = insts[blockIdx.y];
+  hb_ctrl *c = in.ctrl;
   const T *h = (const T *)in.h[c->cur];
   const uint8_t *code = in.code;
+  const int64_t n = (int64_t)in.rows * in.cols;
   double v = 0;
-  for (int64_t k = threadIdx.x; k < (int64_t)in.rows * in.cols; k += blockDim.x) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x) {
     const int r = (int)(k / in.cols), cc = (int)(k - (int64_t)r * in.cols);
     const uint8_t cd = code[(size_t)(r + HB_PAD_Y) * in.code_pitch + cc + HB_CODE_PAD_X];
     if ((cd >> 4) != HB_NODATA_CLASS) v += (double)h[(size_t)(r + HB_PAD_Y) * in.pitch + cc + HB_PAD_X];
@@ -1366,12 +1387,11 @@ prepare_kernel(const hb_instance *__restrict__ insts, BcTable *__restrict__ bct)
   if (threadIdx.x == 0) {
     double V = 0;
     for (int w = 0; w < kNT / 32; w++) V += red[w];
-    c->volume = V * in.dx * in.dx;
-    c->volume0 = c->volume;
-    c->tiles_done = 0u;
-    c->rain_rate = rain_rate_at(in, c, c->t);
-    bc_values_exact(in, c->t, &bct[blockIdx.x]);
-    bc_values_at(in, c, c->t);
+    if (V != 0.0) {
+      V *= in.dx * in.dx;
+      atomicAdd(&c->volume, V);
+      atomicAdd(&c->volume0, V);
+    }
   }
 }
 
@@ -1543,10 +1563,25 @@ int prepare_impl(const hb_fused_batch *b, cudaStream_t st, CUtensorMap *host_map
     if (rc) return rc;
   }
   BcTable *bct = reinterpret_cast<BcTable *>((char *)b->workspace + ws_partials_bytes(b->n_tiles));
-  if (b->dtype == HB_F64)
-    prepare_kernel<double><<<b->n_instances, kNT, 0, st>>>(b->instances, bct);
-  else
-    prepare_kernel<float><<<b->n_instances, kNT, 0, st>>>(b->instances, bct);
+  // blocks per instance for the volume sum: about 16 cells per thread of the
+  // largest instance (the host copy of the records gives the sizes)
+  int64_t most = (int64_t)1 << 22;
+  if (b->instances_host) {
+    most = 0;
+    for (int i = 0; i < b->n_instances; i++)
+      most = std::max<int64_t>(most, (int64_t)b->instances_host[i].rows *
+                                         b->instances_host[i].cols);
+  }
+  const int chunks = (int)std::min<int64_t>(std::max<int64_t>((most + 16 * kNT - 1) /
+                                                                  (16 * kNT), 1), 1024);
+  const dim3 vgrid(chunks, b->n_instances);
+  if (b->dtype == HB_F64) {
+    prepare_kernel<double><<<b->n_instances, 32, 0, st>>>(b->instances, bct);
+    prepare_volume_kernel<double><<<vgrid, kNT, 0, st>>>(b->instances);
+  } else {
+    prepare_kernel<float><<<b->n_instances, 32, 0, st>>>(b->instances, bct);
+    prepare_volume_kernel<float><<<vgrid, kNT, 0, st>>>(b->instances);
+  }
   return check_launch("hb_fused_prepare");
 }
 

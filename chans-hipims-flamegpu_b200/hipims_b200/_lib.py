@@ -86,7 +86,7 @@ class HbAdjointArgs(ctypes.Structure):
         ("out_h", c_vp), ("out_qx", c_vp), ("out_qy", c_vp),
         ("mu", c_vp), ("mu_stride", c_i64), ("grad", c_vp),
         ("t", c_dbl), ("dt", c_dbl), ("rain_rate", c_dbl), ("rain_base", c_dbl),
-        ("first", c_i32), ("pad", c_i32),
+        ("h_reg", c_dbl), ("first", c_i32), ("pad", c_i32),
     ]
 
 

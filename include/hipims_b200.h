@@ -174,6 +174,10 @@ typedef struct hb_adjoint_args {
   double t, dt;                       /* time and time step of step n */
   double rain_rate;                   /* rain rate used by step n (m/s) */
   double rain_base;                   /* the same without the multiplier */
+  double h_reg;                       /* cells with h^n < h_reg get no state adjoint
+                                         (films of a few h_small between deeper cells
+                                         have unstable linearisations; 0 masks only
+                                         negative depths) */
   int32_t first;                      /* step n starts at t == 0 */
   int32_t pad;
 } hb_adjoint_args;

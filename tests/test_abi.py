@@ -56,6 +56,17 @@ def test_fused_rejects_bad_record():
     assert L.hb_fused_workspace_size(None) == 0
 
 
+def test_adjoint_rejects_bad_arguments():
+    L = _lib.lib()
+    a = _lib.HbAdjointArgs()
+    assert ctypes.sizeof(a) == 168
+    assert L.hb_adjoint_step(ctypes.byref(a), None) == -1
+    assert b"null" in L.hb_last_error()
+    assert L.hb_adjoint_gauge(-1, None, None, None, None, 1.0, None) == -1
+    assert L.hb_adjoint_gauge(0, None, None, None, None, 1.0, None) == 0
+    assert L.hb_adjoint_gauge(3, None, None, None, None, 1.0, None) == -1
+
+
 def test_dropin_modules_have_reference_names():
     import euler_update
     import fluxCal_2ndOrder_jh_improved
