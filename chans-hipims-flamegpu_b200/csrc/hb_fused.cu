@@ -1217,6 +1217,19 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
           }
         }
         hu += rain * dt;
+        if (active && in.cum) {
+          // Green-Ampt infiltration on the flux list, after rain
+          // (HC/infiltrationCUDA_Kernel.cu:20-46; order HP/CatchFlood_main.py:164-170)
+          T *cum = (T *)in.cum + (size_t)(ry + HB_PAD_Y) * P + (rx + HB_PAD_X);
+          const int zc = kC & 15;
+          const T K = (T)in.ks[zc], psi = (T)in.psi[zc], dth = (T)in.dtheta[zc];
+          const T F0 = *cum;
+          const T a = F0 + dt * K;
+          const T F1 = T(0.5) * (a + sqrt(a * a + T(4) * dt * K * (psi + hc) * dth));
+          const T dF = fmin(hc, F1 - F0);
+          *cum = F0 + dF;
+          hu -= dF;
+        }
         T h = hc + hu;
         T qx = cC.qx, qy = cC.qy;
         T sgh = T(0);
@@ -1561,6 +1574,11 @@ int prepare_impl(const hb_fused_batch *b, cudaStream_t st, CUtensorMap *host_map
       rc = encode_maps(b, st, maps.data());
     }
     if (rc) return rc;
+  }
+  if (!uses_rows_kernel(b) && b->instances_host) {
+    for (int i = 0; i < b->n_instances; i++)
+      if (b->instances_host[i].cum)
+        return set_error(HB_ERR_ARG, "hb_fused_prepare: infiltration needs the rows kernel");
   }
   BcTable *bct = reinterpret_cast<BcTable *>((char *)b->workspace + ws_partials_bytes(b->n_tiles));
   // blocks per instance for the volume sum: about 16 cells per thread of the

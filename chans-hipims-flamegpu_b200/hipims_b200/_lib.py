@@ -62,6 +62,8 @@ class HbInstance(ctypes.Structure):
         ("bc_type", c_i32 * HB_MAX_CLASSES), ("bc_id", c_i32 * HB_MAX_CLASSES),
         ("n_valid", c_i64),
         ("dt_replay", c_vp), ("n_replay", c_i64),
+        ("cum", c_vp), ("ks", c_dbl * HB_MAX_ZONES), ("psi", c_dbl * HB_MAX_ZONES),
+        ("dtheta", c_dbl * HB_MAX_ZONES),
     ]
 
 

@@ -18,6 +18,7 @@ from __future__ import annotations
 import ctypes
 import dataclasses
 import math
+import os
 from typing import Sequence
 
 import numpy as np
@@ -53,6 +54,9 @@ class Catchment:
     given_q: np.ndarray | None = None       # [Tq, 1 + 2 nQ]
     h_max: np.ndarray | None = None         # default: h
     dt_replay: np.ndarray | None = None     # frozen schedule: dt of step k+1 = dt_replay[k]
+    # Green-Ampt infiltration: {"ks", "psi", "dtheta"} per Manning zone (m/s, m, -)
+    infiltration: dict | None = None
+    cum: np.ndarray | None = None           # initial cumulative infiltrated depth (m)
 
 
 def _round_up(x: int, m: int) -> int:
@@ -144,6 +148,19 @@ class _Instance:
         self.rain = None if c.rain is None else table(c.rain, 2)
         self.dt_replay = None if c.dt_replay is None else torch.as_tensor(
             np.asarray(c.dt_replay, dtype=np.float64), device=device).contiguous()
+        self.cum = None
+        self.infil = None
+        if c.infiltration is not None:
+            self.cum = dense(c.cum)
+            self.initial_cum = self.cum.clone()
+
+            def per_zone(key):
+                v = [float(x) for x in np.atleast_1d(c.infiltration[key])]
+                if len(v) > _lib.HB_MAX_ZONES:
+                    raise ValueError(f"at most {_lib.HB_MAX_ZONES} infiltration zones")
+                return v + [0.0] * (_lib.HB_MAX_ZONES - len(v))
+
+            self.infil = {k: per_zone(k) for k in ("ks", "psi", "dtheta")}
 
         # position of compacted cell 0 (fluxMask quirk)
         if self.n_valid:
@@ -229,6 +246,14 @@ class FusedSolver:
             if ins.dt_replay is not None:
                 r.dt_replay = ins.dt_replay.data_ptr()
                 r.n_replay = ins.dt_replay.numel()
+            if ins.cum is not None:
+                if kernel == "tasks":
+                    raise ValueError("infiltration needs the rows kernel")
+                r.cum = ins.cum.data_ptr()
+                for z_ in range(_lib.HB_MAX_ZONES):
+                    r.ks[z_] = ins.infil["ks"][z_]
+                    r.psi[z_] = ins.infil["psi"][z_]
+                    r.dtheta[z_] = ins.infil["dtheta"][z_]
             nt = ins.tiles_x * ins.tiles_y
             tile_inst.extend([k] * nt)
             begin += nt
@@ -289,6 +314,8 @@ class FusedSolver:
                 ins.qx[buf].copy_(qx0)
                 ins.qy[buf].copy_(qy0)
             ins.h_max.copy_(ins.initial_h_max)
+            if ins.cum is not None:
+                ins.cum.copy_(ins.initial_cum)
         self.ctrl.copy_(torch.frombuffer(bytearray(arr), dtype=torch.uint8))
         self.prepare()
 
@@ -378,6 +405,8 @@ class FusedSolver:
         ins = self.inst[k]
         out = {"h": ins.raster(ins.h[cur]), "qx": ins.raster(ins.qx[cur]),
                "qy": ins.raster(ins.qy[cur]), "h_max": ins.raster(ins.h_max)}
+        if ins.cum is not None:
+            out["cum"] = ins.raster(ins.cum)
         z = ins.raster(ins.z).double().cpu().numpy() + ins.z_abs_offset
         out["z"] = torch.as_tensor(z)
         return out
@@ -388,6 +417,84 @@ class FusedSolver:
         v = self.inst[k].valid
         return {name: (t.cpu().numpy() if torch.is_tensor(t) else t)[v].astype(np.float64)
                 for name, t in st.items()}
+
+    # ------------------------------------------------------ export / checkpoint
+    def time_tag(self, k: int = 0) -> str:
+        """The reference's export file tag: str() of the time as a 1-element
+        device tensor of the run's dtype (HP/SWE_CUDA.py:836-868 names files
+        <field>_<str(t + dt)>.pt; post-processing globs 'h_tensor*.pt')."""
+        t = self.controls()[k].t
+        return str(torch.tensor([t], dtype=self.dtype, device=self.device))
+
+    def export_fields(self, outpath: str, k: int = 0) -> list[str]:
+        """Write h, qx, qy, wl and h_max of instance k as the reference's
+        exportField does: compacted (row-major valid-cell order) tensors of the
+        run's dtype on the device, one <field>_<tag>.pt file each."""
+        ins = self.inst[k]
+        st = self.state(k)
+        valid = torch.as_tensor(ins.valid, device=self.device)
+        z_abs = torch.as_tensor(st["z"], dtype=torch.float64, device=self.device)
+        fields = {"h": st["h"], "qx": st["qx"], "qy": st["qy"],
+                  "wl": (st["h"].double() + z_abs).to(self.dtype), "h_max": st["h_max"]}
+        os.makedirs(outpath, exist_ok=True)
+        tag = self.time_tag(k)
+        paths = []
+        for name, x in fields.items():
+            p = os.path.join(outpath, f"{name}_{tag}.pt")
+            torch.save(x[valid].contiguous(), p)
+            paths.append(p)
+        return paths
+
+    def checkpoint(self) -> dict:
+        """Device copy of everything a restart needs: each instance's current
+        state and h_max, and the control blocks (t, dt, step, export counter,
+        rain cursor, volume / rain / outflow totals)."""
+        cs = self.controls()
+        inst = []
+        for k, ins in enumerate(self.inst):
+            cur = cs[k].cur
+            inst.append({"rows": ins.rows, "cols": ins.cols, "n_valid": ins.n_valid,
+                         "h": ins.h[cur].clone(), "qx": ins.qx[cur].clone(),
+                         "qy": ins.qy[cur].clone(), "h_max": ins.h_max.clone(),
+                         "cum": None if ins.cum is None else ins.cum.clone()})
+        return {"dtype": str(self.dtype), "ctrl": self.ctrl.clone(), "instances": inst}
+
+    def restore(self, ckpt: dict) -> None:
+        """Resume from checkpoint(): same catchments, same dtype."""
+        if ckpt["dtype"] != str(self.dtype) or len(ckpt["instances"]) != len(self.inst):
+            raise ValueError("checkpoint does not match this solver (dtype or instances)")
+        saved = (_lib.HbCtrl * len(self.inst)).from_buffer_copy(
+            bytearray(ckpt["ctrl"].cpu().numpy().tobytes()))
+        for k, (ins, rec) in enumerate(zip(self.inst, ckpt["instances"])):
+            if (rec["rows"], rec["cols"], rec["n_valid"]) != (ins.rows, ins.cols, ins.n_valid):
+                raise ValueError(f"checkpoint instance {k} has another raster")
+            cur = saved[k].cur
+            ins.h[cur].copy_(rec["h"])
+            ins.qx[cur].copy_(rec["qx"])
+            ins.qy[cur].copy_(rec["qy"])
+            ins.h_max.copy_(rec["h_max"])
+            if (ins.cum is None) != (rec.get("cum") is None):
+                raise ValueError(f"checkpoint instance {k} differs in infiltration")
+            if ins.cum is not None:
+                ins.cum.copy_(rec["cum"])
+        self.ctrl.copy_(ckpt["ctrl"].to(self.device))
+        self.prepare()  # boundary tables and rain rate at t; resets the volume baseline
+        cs = self.controls()
+        for k, c in enumerate(cs):
+            c.volume0 = saved[k].volume0
+        self.write_controls(cs)
+
+    def save_checkpoint(self, path: str) -> None:
+        ck = self.checkpoint()
+        ck["ctrl"] = ck["ctrl"].cpu()
+        for rec in ck["instances"]:
+            for f in ("h", "qx", "qy", "h_max", "cum"):
+                if rec[f] is not None:
+                    rec[f] = rec[f].cpu()
+        torch.save(ck, path)
+
+    def load_checkpoint(self, path: str) -> None:
+        self.restore(torch.load(path, map_location="cpu", weights_only=False))
 
     def cell_offsets(self, k: int, rows: np.ndarray, cols: np.ndarray) -> torch.Tensor:
         """Flat element offsets of raster cells in the dense state arrays (for gather)."""

@@ -99,6 +99,13 @@ typedef struct hb_instance {
   int64_t n_valid;           /* valid cells */
   const double *dt_replay;   /* optional: dt of step k+1 is dt_replay[k] for k < n_replay */
   int64_t n_replay;          /* (frozen time-step schedule; 0 = adaptive CFL step) */
+  /* optional Green-Ampt infiltration (HC/infiltrationCUDA_Kernel.cu:20-46), applied
+   * to the active cells after rain as HP/CatchFlood_main.py:164-170 orders it;
+   * cum = NULL disables it.  Rows kernel only. */
+  void *cum;                 /* cumulative infiltrated depth, dense like h (in place) */
+  double ks[HB_MAX_ZONES];   /* saturated hydraulic conductivity per zone (m/s) */
+  double psi[HB_MAX_ZONES];  /* capillary head per zone (m) */
+  double dtheta[HB_MAX_ZONES]; /* water-content difference per zone */
 } hb_instance;
 
 /* Launch record (host memory). */

@@ -546,12 +546,15 @@ typedef void (*or_ref_timestep_fn)(int, int32_t *, double *, double *, double *,
                                    double *);
 typedef void (*or_ref_rain_fn)(int, double *, int16_t *, double *, double *);
 typedef void (*or_ref_mask_fn)(int, uint8_t *, double *, const int32_t *, double *);
+typedef void (*or_ref_infil_fn)(int, int32_t *, double *, uint8_t *, double *, double *,
+                                double *, double *, double *, double *);
 typedef struct {
   or_ref_flux_fn flux2, flux1;
   or_ref_friction_fn friction;
   or_ref_timestep_fn timestep;
   or_ref_rain_fn rain;
   or_ref_mask_fn mask;
+  or_ref_infil_fn infil;
 } or_ref_kernels;
 
 typedef struct {
@@ -582,6 +585,10 @@ typedef struct {
   uint8_t *fmask;
   double *accel;
   const or_ref_kernels *ref; /* NULL: use the restatement */
+  /* Green-Ampt infiltration (NULL cum: none): per-zone K_s, capillary head,
+   * water-content difference; per-cell cumulative infiltrated depth */
+  const double *ks, *psi, *dtheta;
+  double *cum;
 } or_godunov;
 
 /* Rain table interpolation with the reference's monotone row cursor.
@@ -645,6 +652,16 @@ void or_godunov_step(or_godunov *s) {
       double rdt = s->rain_rate[0] * s->dt;
       for (int64_t i = 0; i < N; i++) s->h_upd[i] += rdt;
     }
+  }
+  /* infiltration on the flux list (HP/CatchFlood_main.py:164-170 order:
+   * addFlux, rain, addInfiltrationSource, friction; HP/SWE_CUDA.py:439-443) */
+  if (s->cum && M > 0) {
+    if (k && k->infil)
+      k->infil((int)M, s->list, s->h_upd, (uint8_t *)s->landuse, s->h, (double *)s->ks,
+               (double *)s->psi, (double *)s->dtheta, s->cum, &dt0);
+    else
+      or_infiltration(M, s->list, s->h_upd, s->landuse, s->h, s->ks, s->psi, s->dtheta,
+                      s->cum, s->dt);
   }
   /* time_friction_euler_update_cuda */
   double time_upper = s->dt * 10.0;

@@ -146,7 +146,7 @@ def infiltration(wet, hu, landuse, h, ks, psi, dth, cum, dt):
 # ------------------------------------------------------------------ driver
 class _RefKernels(ctypes.Structure):
     _fields_ = [("flux2", _P), ("flux1", _P), ("friction", _P), ("timestep", _P),
-                ("rain", _P), ("mask", _P)]
+                ("rain", _P), ("mask", _P), ("infil", _P)]
 
 
 class _Godunov(ctypes.Structure):
@@ -162,6 +162,7 @@ class _Godunov(ctypes.Structure):
         ("rain", _P), ("rain_rows", _I), ("rain_cols", _I),
         ("rain_mask", _P), ("rain_index", _I), ("rain_rate", _P), ("exports", _I),
         ("list", _P), ("fmask", _P), ("accel", _P), ("ref", _P),
+        ("ks", _P), ("psi", _P), ("dtheta", _P), ("cum", _P),
     ]
 
 
@@ -170,8 +171,9 @@ class Sim:
 
     d: dict with mask, z, h, qx, qy, (wl), landuse, manning, dx, cfl, first_dt
     and optional rain [T, 1+S], rain_mask raster, given_depth/given_wl/given_q,
-    export_step, t0.  backend: "oracle" (restatement) or "ref" (the reference
-    kernels built for the host).
+    export_step, t0, infiltration = {"ks", "psi", "dtheta": per-zone lists,
+    "cum": optional initial cumulative depth raster}.  backend: "oracle"
+    (restatement) or "ref" (the reference kernels built for the host).
     """
 
     def __init__(self, d: dict, order: int = 2, backend: str = "oracle",
@@ -228,13 +230,23 @@ class Sim:
         if self.rain is not None:
             g.rain, (g.rain_rows, g.rain_cols) = self.rain.ctypes.data, self.rain.shape
         g.rain_mask = _p(self.rain_mask)
+        inf = d.get("infiltration")
+        self.cum = None
+        if inf is not None:
+            par = lambda a: np.ascontiguousarray(np.atleast_1d(np.asarray(a, np.float64)))
+            self.ks, self.psi, self.dtheta = par(inf["ks"]), par(inf["psi"]), par(inf["dtheta"])
+            self.cum = (np.zeros(N) if inf.get("cum") is None else f64(inf["cum"])).copy()
+            g.ks, g.psi, g.dtheta = (self.ks.ctypes.data, self.psi.ctypes.data,
+                                     self.dtheta.ctypes.data)
+            g.cum = self.cum.ctypes.data
         self._kern = None
         if backend == "ref":
             R = ref_lib()
             k = _RefKernels()
             for f, sym in (("flux2", "ref_flux2"), ("flux1", "ref_flux1"),
                            ("friction", "ref_friction_update"), ("timestep", "ref_timestep"),
-                           ("rain", "ref_rain_station"), ("mask", "ref_flux_mask")):
+                           ("rain", "ref_rain_station"), ("mask", "ref_flux_mask"),
+                           ("infil", "ref_infiltration")):
                 setattr(k, f, ctypes.cast(getattr(R, sym), _P).value)
             self._kern = k
             g.ref = ctypes.addressof(k)
@@ -274,5 +286,8 @@ class Sim:
         return np.asarray(dts)
 
     def state(self) -> dict:
-        return dict(h=self.h.copy(), qx=self.qx.copy(), qy=self.qy.copy(), wl=self.wl.copy(),
-                    h_max=self.h_max.copy(), t=self.g.t, dt=self.g.dt)
+        st = dict(h=self.h.copy(), qx=self.qx.copy(), qy=self.qy.copy(), wl=self.wl.copy(),
+                  h_max=self.h_max.copy(), t=self.g.t, dt=self.g.dt)
+        if self.cum is not None:
+            st["cum"] = self.cum.copy()
+        return st

@@ -71,6 +71,10 @@ def cases() -> dict:
     out["channel_o1"] = (c1, 1)
     out["mixed_bc_o2"] = (mixed_bc_case(11, 2), 2)
     out["mixed_bc_o1"] = (mixed_bc_case(12, 1), 1)
+    u = S.urban_catchment(24, dx=2.0, seed=9)
+    u.update(steps=200, infiltration=dict(ks=[2.0e-6, 5.0e-6], psi=[0.11, 0.2],
+                                          dtheta=[0.3, 0.45]))
+    out["urban24_infil_o2"] = (u, 2)
     return out
 
 
@@ -86,7 +90,10 @@ def run_case(d: dict, order: int, backend: str) -> tuple[dict, int]:
 def main() -> None:
     if not O.ref_available():
         raise SystemExit("oracle/_ref is not built: python oracle/build_ref.py")
+    only = set(sys.argv[1:])
     for name, (d, order) in cases().items():
+        if only and name not in only:
+            continue
         st, n = run_case(d, order, "ref")
         payload = {k: np.asarray(d[k]) for k in KEYS if d.get(k) is not None}
         for k in ("manning", "rain", "given_depth", "given_wl", "given_q"):
@@ -97,8 +104,12 @@ def main() -> None:
                     export_step=d.get("export_step", 1.0e30))
         for k, v in scal.items():
             payload["in_" + k] = np.asarray(v, dtype=np.float64)
-        for k in ("h", "qx", "qy", "wl", "h_max"):
-            payload["out_" + k] = st[k]
+        if d.get("infiltration") is not None:
+            for k in ("ks", "psi", "dtheta"):
+                payload["infil_" + k] = np.asarray(d["infiltration"][k], dtype=np.float64)
+        for k in ("h", "qx", "qy", "wl", "h_max", "cum"):
+            if k in st:
+                payload["out_" + k] = st[k]
         payload["out_t"] = np.asarray(st["t"])
         payload["out_dt"] = np.asarray(st["dt"])
         payload["out_steps"] = np.asarray(n)
@@ -118,6 +129,8 @@ def load_case(path: str) -> tuple[dict, int, dict]:
     for k in ("dx", "cfl", "first_dt", "steps", "t_end", "export_step"):
         d[k] = float(z["in_" + k])
     d["steps"] = int(d["steps"])
+    if "infil_ks" in z.files:
+        d["infiltration"] = {k: z["infil_" + k] for k in ("ks", "psi", "dtheta")}
     order = int(z["in_order"])
     exp = {k[4:]: z[k] for k in z.files if k.startswith("out_")}
     return d, order, exp

@@ -6,6 +6,7 @@ FP32 fused: compared with the FP64 oracle at identical simulated times (the
 oracle's dt sequence is replayed) with the north-star tolerance, max depth
 error <= 1e-4 m; the adaptive FP32 run is checked too."""
 import math
+import os
 
 import numpy as np
 import pytest
@@ -218,3 +219,109 @@ def test_fused_mass_balance(cuda):
     assert c.outflow_volume > 0
     rel = abs(c.volume - c.volume0 - c.rain_volume + c.outflow_volume) / c.rain_volume
     assert rel < 1e-4, rel
+
+
+def test_checkpoint_restart_is_bitwise(cuda, tmp_path):
+    """Checkpoint after 20 steps, restart in a fresh solver from the saved
+    file: the next 30 steps equal an uninterrupted run bit for bit, and the
+    control block (t, dt, step, export counter, totals) carries over."""
+    from hipims_b200 import scenarios as S
+    from hipims_b200.fused import FusedSolver
+
+    d = S.urban_catchment(96, dx=2.0, seed=3)
+    c = S.catchment_from(d, export_step=30.0)
+    a = FusedSolver(c, dtype=torch.float32, device=cuda)
+    a.step(20)
+    path = str(tmp_path / "ck.pt")
+    a.save_checkpoint(path)
+    a.step(30)
+    b = FusedSolver(c, dtype=torch.float32, device=cuda)
+    b.load_checkpoint(path)
+    b.step(30)
+    sa, sb = a.state(), b.state()
+    for f in ("h", "qx", "qy", "h_max"):
+        assert torch.equal(sa[f], sb[f]), f
+    ca, cb = a.controls()[0], b.controls()[0]
+    for f in ("t", "dt", "step", "export_n", "rain_index", "volume0", "rain_volume",
+              "outflow_volume"):
+        assert getattr(ca, f) == getattr(cb, f), f
+
+
+def test_export_fields_use_reference_names(cuda, tmp_path):
+    """export_fields writes <field>_<str(t tensor)>.pt compacted tensors, the
+    names the reference's post-processing globs for (h_tensor*.pt)."""
+    from hipims_b200 import scenarios as S
+    from hipims_b200.fused import FusedSolver
+
+    d = S.dam_break(32)
+    fs = FusedSolver(S.catchment_from(d, export_step=0.05, halt_on_export=True),
+                     dtype=torch.float64, device=cuda)
+    fs.run_until(1.0)
+    c = fs.controls()[0]
+    assert c.halted and c.exports == 1 and c.t == pytest.approx(0.05, abs=1e-12)
+    paths = fs.export_fields(str(tmp_path))
+    names = sorted(os.path.basename(p) for p in paths)
+    tag = str(torch.tensor([c.t], dtype=torch.float64, device=cuda))
+    assert names == sorted(f"{f}_{tag}.pt" for f in ("h", "qx", "qy", "wl", "h_max"))
+    assert any(n.startswith("h_tensor") for n in names)
+    h = torch.load(os.path.join(str(tmp_path), f"h_{tag}.pt"))
+    np.testing.assert_array_equal(h.cpu().numpy(), fs.compacted()["h"])
+    wl = torch.load(os.path.join(str(tmp_path), f"wl_{tag}.pt"))
+    comp = fs.compacted()
+    np.testing.assert_allclose(wl.cpu().numpy(), comp["h"] + comp["z"], rtol=0, atol=1e-12)
+
+
+INFIL = dict(ks=[2.0e-6, 5.0e-6], psi=[0.11, 0.2], dtheta=[0.3, 0.45])
+
+
+@pytest.mark.parametrize("dtype,steps,tol", [(torch.float64, 200, 1e-9),
+                                             (torch.float32, 200, 1e-4)])
+def test_fused_infiltration_matches_oracle(cuda, dtype, steps, tol):
+    """Green-Ampt infiltration inside the fused step (after rain, on the flux
+    list, as HP/CatchFlood_main.py:164-170 orders it) against the oracle's step
+    with the same source, on a dam break over two soil zones under rain; the
+    oracle's step is pinned to the reference's own infiltration kernel built
+    for the host."""
+    from hipims_b200 import scenarios as S
+    from hipims_b200.fused import FusedSolver
+
+    d = S.dam_break(64)
+    # 1.0 m | 0.3 m, so that infiltration dries no cell (a wet/dry front makes
+    # the FP32 and FP64 trajectories part at the scheme's thresholds)
+    d["h"] = np.where((d["mask"] > 0) & (d["h"] < 0.5), 0.3, d["h"])
+    d["wl"] = d["z"] + d["h"]
+    zone = np.zeros(d["mask"].shape, dtype=np.uint8)
+    zone[:, (3 * zone.shape[1]) // 4:] = 1  # soil zones split across x: the flow stays 1-D
+    d["landuse"] = zone
+    d["manning"] = [0.03, 0.05]
+    d["rain"] = np.array([[0.0, 2.0e-5], [10.0, 2.0e-5]])
+    d["infiltration"] = dict(INFIL)
+    sim = O.Sim(d, order=2)
+    dts = sim.run_record(steps)
+    fs = FusedSolver(catchment(d, infiltration=dict(INFIL), dt_replay=dts), dtype=dtype,
+                     device=cuda)
+    fs.step(steps)
+    got, st = fs.compacted(), sim.state()
+    assert float(np.abs(got["cum"] - st["cum"]).max()) <= tol
+    assert float(np.abs(got["h"] - st["h"]).max()) <= tol
+    assert st["cum"].max() > 1e-6  # the source is active
+
+
+def test_fused_infiltration_reset_and_checkpoint(cuda, tmp_path):
+    from hipims_b200 import scenarios as S
+    from hipims_b200.fused import FusedSolver
+
+    d = S.urban_catchment(48, dx=2.0, seed=6)
+    c = catchment(d, infiltration=dict(INFIL))
+    a = FusedSolver(c, dtype=torch.float32, device=cuda)
+    a.step(15)
+    ck = str(tmp_path / "ck.pt")
+    a.save_checkpoint(ck)
+    a.step(10)
+    b = FusedSolver(c, dtype=torch.float32, device=cuda)
+    b.load_checkpoint(ck)
+    b.step(10)
+    assert torch.equal(a.state()["cum"], b.state()["cum"])
+    assert torch.equal(a.state()["h"], b.state()["h"])
+    a.reset()
+    assert float(a.state()["cum"].abs().max()) == 0.0

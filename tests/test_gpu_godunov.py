@@ -38,10 +38,17 @@ def run_godunov(d, order, dev, steps, t_end=np.inf, export_step=1e30, dtype=torc
     g.set_distributed_rainfall_station_Mask(mask, torch.as_tensor(np.asarray(rm)), dev)
     rain = d.get("rain")
     rain = np.array([[0.0, 0.0], [1e9, 0.0]]) if rain is None else np.asarray(rain)
+    inf = d.get("infiltration")
+    if inf is not None:
+        P = lambda a: torch.as_tensor(np.atleast_1d(np.asarray(a, np.float64)), device=dev)
+        g.set__infiltrationField_tensor(P(inf["ks"]), P(inf["psi"]), P(inf["dtheta"]), dev)
     n = 0
     while n < steps and g.t.item() < t_end:
+        # HP/CatchFlood_main.py:164-170: flux, station rain, infiltration, friction
         g.addFlux()
         g.addStation_PrecipitationSource(rain, dev)
+        if inf is not None:
+            g.addInfiltrationSource()
         g.time_friction_euler_update_cuda(dev)
         n += 1
     return g, n
@@ -52,7 +59,7 @@ def run_godunov(d, order, dev, steps, t_end=np.inf, export_step=1e30, dtype=torc
 # a 1e-16 difference (CUDA vs glibc pow in the friction step) grows to ~1e-6 m
 # within 60 steps, so that case gets a looser final tolerance and a tight
 # check over its first steps.
-GOLDEN_ATOL = {"mixed_bc_o2.npz": 1e-4}
+GOLDEN_ATOL = {"mixed_bc_o2.npz": 1e-4, "urban24_infil_o2.npz": 1e-5}
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
@@ -62,8 +69,11 @@ def test_godunov_matches_reference_outputs(cuda, path):
     assert n == int(exp["steps"])
     atol = GOLDEN_ATOL.get(os.path.basename(path), 1e-10)
     assert g.t.item() == pytest.approx(float(exp["t"]), rel=max(atol, 1e-12))
-    for k, x in (("h", g._h_internal), ("qx", g._qx_internal), ("qy", g._qy_internal),
-                 ("h_max", g._h_max)):
+    fields = [("h", g._h_internal), ("qx", g._qx_internal), ("qy", g._qy_internal),
+              ("h_max", g._h_max)]
+    if "cum" in exp:
+        fields.append(("cum", g._cumulativeWaterDepth))
+    for k, x in fields:
         np.testing.assert_allclose(x.cpu().numpy(), exp[k], rtol=0, atol=atol, err_msg=k)
 
 
