@@ -281,12 +281,16 @@ def run_ours(args) -> None:
         if args.accuracy:
             line["accuracy"] = accuracy_vs_fp64(d, dev)
         if args.plain and world == 1:
-            pl = plain_fp64_rate(d, dev)
-            pl["fused_fp32_over_plain"] = value / pl["value"]
+            pl = plain_fp64_rate(d, dev, reference_kernels=True)
+            if pl.get("value"):
+                pl["fused_fp32_over_plain"] = value / pl["value"]
             line["fp64_plain"] = pl
+            pc = plain_fp64_rate(d, dev, reference_kernels=False)
+            pc["fused_fp32_over_compat"] = value / pc["value"]
+            line["fp64_compat"] = pc
         if args.ensemble and world == 1:
             en = ensemble_rate(dev, args.ensemble_steps)
-            if "fp64_plain" in line:
+            if line.get("fp64_plain", {}).get("value"):
                 en["over_plain_fp64"] = en["value"] / line["fp64_plain"]["value"]
             line["ensemble"] = en
         if args.adjoint and world == 1:
@@ -302,14 +306,26 @@ def run_ours(args) -> None:
     del _lib
 
 
-def plain_fp64_rate(d: dict, dev, steps: int = 5) -> dict:
+def plain_fp64_rate(d: dict, dev, steps: int = 5, reference_kernels: bool = True) -> dict:
     """The plain FP64 GPU path: the reference solver loop (Godunov object API,
     compacted cells, gather-based per-cell fluxes, host syncs per step) on the
-    compat ops, on the same catchment, wall-clock per step."""
+    same catchment, wall-clock per step; with reference_kernels the ops are the
+    reference's own kernels built for sm_100a (baseline/build_ref_cuda.py),
+    else this library's compat ops."""
     from hipims_b200.solver import Godunov
 
+    impl, path = None, "Godunov loop on the compat ops (reference kernel structure), wall clock"
+    if reference_kernels:
+        from baseline import ref_gpu
+
+        if not ref_gpu.available():
+            return {"value": None, "unavailable": "baseline/_ref not built"}
+        impl = ref_gpu.RefGpuOps()
+        path = ("Godunov loop on the reference's own kernels built for sm_100a "
+                "(flux, fluxMask, friction-update, timeControl, station rain), torch.min, "
+                "wall clock")
     g = Godunov(dev, d["dx"], d["cfl"], 1.0e30, secondOrder=True,
-                firstTimeStep=d["first_dt"], tensorType=torch.float64)
+                firstTimeStep=d["first_dt"], tensorType=torch.float64, ops_impl=impl)
     g._export_enabled = False
     T = lambda a: torch.as_tensor(np.asarray(a, dtype=np.float64))
     mask = torch.as_tensor(d["mask"])
@@ -334,7 +350,7 @@ def plain_fp64_rate(d: dict, dev, steps: int = 5) -> dict:
     el = time.perf_counter() - t0
     n = int(g._h_internal.numel())
     return {"value": n * steps / el / 1e9, "unit": METRIC, "steps": steps, "dtype": "f64",
-            "path": "Godunov loop on the compat ops (reference kernel structure), wall clock"}
+            "path": path}
 
 
 def ensemble_rate(dev, steps: int, count: int = 64, seed: int = 0) -> dict:

@@ -1137,6 +1137,8 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
     T *qyout = (T *)in.qy[1 - cur];
     T *hmaxg = (T *)in.h_max;
     const int rx = x0 + j;
+    // read once per tile: the state stores below may alias the record
+    const bool infil = in.cum != nullptr;
 
 #pragma unroll 1
     for (int i = r0; i < r0 + R; ++i) {
@@ -1217,7 +1219,7 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
           }
         }
         hu += rain * dt;
-        if (active && in.cum) {
+        if (infil && active) {
           // Green-Ampt infiltration on the flux list, after rain
           // (HC/infiltrationCUDA_Kernel.cu:20-46; order HP/CatchFlood_main.py:164-170)
           T *cum = (T *)in.cum + (size_t)(ry + HB_PAD_Y) * P + (rx + HB_PAD_X);

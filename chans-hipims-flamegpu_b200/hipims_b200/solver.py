@@ -28,7 +28,11 @@ from .topology import compact_index
 
 class Godunov:
     def __init__(self, device, dx, CFL, Export_timeStep, t=0.0, export_n=0,
-                 secondOrder=False, firstTimeStep=1.0e-4, tensorType=torch.float64):
+                 secondOrder=False, firstTimeStep=1.0e-4, tensorType=torch.float64,
+                 ops_impl=None):
+        # ops_impl: an object with the op functions of hipims_b200.ops (default),
+        # so that the same loop can drive another implementation of the ops
+        self._ops = ops if ops_impl is None else ops_impl
         self._tensorType = tensorType
         self._secondOrder = secondOrder
         self._device = torch.device(device)
@@ -125,18 +129,19 @@ class Godunov:
     def addFlux(self):
         """fluxMask -> active list -> HLLC flux accumulation (HP/SWE_CUDA.py:339-424)."""
         fm = torch.zeros_like(self._h_internal, dtype=torch.bool)
-        ops.flux_mask(fm, self._h_internal, self._index, self.t)
+        self._ops.flux_mask(fm, self._h_internal, self._index, self.t)
         self._wetMask = torch.flatten(fm.nonzero()).to(torch.int32)
-        op = ops.flux_2nd_order if self._secondOrder else ops.flux_1st_order
+        op = self._ops.flux_2nd_order if self._secondOrder else self._ops.flux_1st_order
         op(self._wetMask, self._h_update, self._qx_update, self._qy_update, self._h_internal,
            self._wl_internal, self._z_internal, self._qx_internal, self._qy_internal,
            self._index, self._normal, self._given_depth, self._given_wl,
            self._given_discharge, self.dx, self.t, self.dt)
 
     def addInfiltrationSource(self):
-        ops.infiltration(self._wetMask, self._h_update, self._landuseMask, self._h_internal,
-                         self._hydraulic_conductivity, self._capillary_head,
-                         self._water_content_diff, self._cumulativeWaterDepth, self.dt)
+        self._ops.infiltration(self._wetMask, self._h_update, self._landuseMask,
+                               self._h_internal, self._hydraulic_conductivity,
+                               self._capillary_head, self._water_content_diff,
+                               self._cumulativeWaterDepth, self.dt)
 
     def _interp_rain(self, R: np.ndarray) -> np.ndarray:
         """Rain rates at t with the monotone row cursor (HP/SWE_CUDA.py:472-495)."""
@@ -152,8 +157,8 @@ class Godunov:
     def addStation_PrecipitationSource(self, rainfall_ndarray_data, device):
         rates = self._interp_rain(np.asarray(rainfall_ndarray_data, dtype=np.float64))
         self._rainStationData = torch.as_tensor(rates, dtype=self._tensorType, device=device)
-        ops.station_rain(self._h_update, self._rainfall_station_Mask, self._rainStationData,
-                         self.dt)
+        self._ops.station_rain(self._h_update, self._rainfall_station_Mask,
+                               self._rainStationData, self.dt)
 
     def add_uniform_PrecipitationSource(self, rainfall_ndarray_data, device):
         rates = self._interp_rain(np.asarray(rainfall_ndarray_data, dtype=np.float64))
@@ -169,15 +174,15 @@ class Godunov:
 
     def friction_euler_update_cuda(self):
         self._wetMask = self._update_list()
-        ops.friction_update(self._wetMask, self._h_update, self._qx_update, self._qy_update,
-                            self._z_update, self._landuseMask, self._h_internal,
-                            self._wl_internal, self._qx_internal, self._qy_internal,
-                            self._z_internal, self._manning, self.dt)
+        self._ops.friction_update(self._wetMask, self._h_update, self._qx_update,
+                                  self._qy_update, self._z_update, self._landuseMask,
+                                  self._h_internal, self._wl_internal, self._qx_internal,
+                                  self._qy_internal, self._z_internal, self._manning, self.dt)
 
     def _advance_dt(self, time_upper: torch.Tensor, listed: int) -> None:
         """min -> 10x cap -> export clip -> t += dt (HP/SWE_CUDA.py:818-831)."""
         if listed != 0:
-            self.dt = ops.device_min(self._accelerator_dt)
+            self.dt = self._ops.device_min(self._accelerator_dt)
         self.dt = torch.where(time_upper < self.dt, time_upper, self.dt)
         nxt = float(self._export_n + 1) * self.export_timeStep
         if (self.dt + self.t).item() >= nxt:
@@ -191,17 +196,18 @@ class Godunov:
         self.friction_euler_update_cuda()
         self._accelerator_dt = torch.full(self._wetMask.size(), self._maxTimeStep.item(),
                                           dtype=self._tensorType, device=device)
-        ops.update_timestep(self._wetMask, self._accelerator_dt, self._h_max, self._h_internal,
-                            self._qx_internal, self._qy_internal, self.dx, self.cfl, self.t,
-                            self.dt)
+        self._ops.update_timestep(self._wetMask, self._accelerator_dt, self._h_max,
+                                  self._h_internal, self._qx_internal, self._qy_internal,
+                                  self.dx, self.cfl, self.t, self.dt)
         self._advance_dt(time_upper, self._accelerator_dt.size(0))
 
     def euler_update(self):
         self._wetMask = torch.flatten(((self._h_update.abs() > 0.0) |
                                        (self._h_internal > 1.0e-6)).nonzero()).to(torch.int32)
-        ops.euler_update(self._wetMask, self._h_update, self._qx_update, self._qy_update,
-                         self._z_update, self._h_internal, self._wl_internal,
-                         self._z_internal, self._qx_internal, self._qy_internal)
+        self._ops.euler_update(self._wetMask, self._h_update, self._qx_update,
+                               self._qy_update, self._z_update, self._h_internal,
+                               self._wl_internal, self._z_internal, self._qx_internal,
+                               self._qy_internal)
         self._h_update.zero_()
         self._qx_update.zero_()
         self._qy_update.zero_()
@@ -212,9 +218,9 @@ class Godunov:
         self._wetMask = torch.flatten((self._h_internal > 1.0e-6).nonzero()).to(torch.int32)
         self._accelerator_dt = torch.full(self._wetMask.size(), self._maxTimeStep.item(),
                                           dtype=self._tensorType, device=device)
-        ops.update_timestep(self._wetMask, self._accelerator_dt, self._h_max, self._h_internal,
-                            self._qx_internal, self._qy_internal, self.dx, self.cfl, self.t,
-                            self.dt)
+        self._ops.update_timestep(self._wetMask, self._accelerator_dt, self._h_max,
+                                  self._h_internal, self._qx_internal, self._qy_internal,
+                                  self.dx, self.cfl, self.t, self.dt)
         self._advance_dt(time_upper, self._accelerator_dt.size(0))
 
     def rungeKutta_update(self, rainfallMatrix, device):
