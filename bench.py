@@ -155,6 +155,25 @@ def cpu_reference_rate(d: dict, steps: int, warmup: int, threads: int | None = N
                       f"{SPINUP + warmup} untimed steps, FP64, {threads} threads"}
 
 
+def cpu_dam_break_rates(steps: int = 1000) -> dict:
+    """Config 1 on the host: the 256 x 256 dam break, 1000 FP64 steps of the
+    reference's kernels built for the host, with 1 thread and with all."""
+    from hipims_b200 import scenarios as S
+    from oracle import oracle as O
+
+    kind = "reference" if O.ref_available() else "port"
+    out = {"kind": kind, "steps": steps, "cells": 256 * 256}
+    for threads in (1, os.cpu_count() or 1):
+        O.set_threads(threads)
+        sim = O.Sim(S.dam_break(256), order=2, backend="ref" if kind == "reference" else "oracle")
+        t0 = time.perf_counter()
+        sim.run(steps)
+        el = time.perf_counter() - t0
+        out[f"threads_{threads}"] = {"value": sim.N * steps / el / 1e9, "unit": METRIC,
+                                     "seconds": el}
+    return out
+
+
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -293,8 +312,13 @@ def run_ours(args) -> None:
             if line.get("fp64_plain", {}).get("value"):
                 en["over_plain_fp64"] = en["value"] / line["fp64_plain"]["value"]
             line["ensemble"] = en
+        if args.coupled and world == 1:
+            line["coupled"] = coupled_rate(dev, args.coupled_cells, tile=tuple(args.tile),
+                                           minb=args.minb)
         if args.adjoint and world == 1:
             line["adjoint"] = adjoint_cost(dev, args.adjoint_cells, args.adjoint_steps)
+        if args.cpu_c1 and world == 1:
+            line["cpu_dam_break"] = cpu_dam_break_rates()
         if args.cpu_baseline and world == 1:
             line["cpu_baseline"] = {k: v for k, v in cpu_reference_rate(
                 d, args.cpu_steps, 0).items() if k in ("value", "unit", "cores", "kind",
@@ -457,6 +481,55 @@ def adjoint_cost(dev, n: int = 1024, steps: int = 2000, K: int = 100, every: int
     return out
 
 
+def coupled_rate(dev, n: int = 8192, sim_seconds: float = 120.0, period: float = 60.0,
+                 agents: int = 100_000, tile=(32, 32), minb: int = 5) -> dict:
+    """Config 5: an n x n catchment (1 m cells, rain 100 mm/h, Q_GIVEN inflow
+    hydrograph on one edge) advanced by the fused FP32 step from a dry start;
+    every `period` simulated seconds the agent cells' depth and velocities are
+    gathered on the device, copied to the host and serialised with msgpack, as
+    the RPC server's request_data answer.  Wall clock over the whole run."""
+    import msgpack
+
+    from hipims_b200 import scenarios as S
+    from hipims_b200.coupling import FusedBackend
+    from hipims_b200.fused import FusedSolver
+    from hipims_b200.scenarios import catchment_from
+
+    d = S.coupled_case(n, agents=agents)
+    fs = FusedSolver(catchment_from(d, t_end=sim_seconds), dtype=torch.float32,
+                     tile=tuple(tile), device=dev, minb=minb)
+    be = FusedBackend(fs, d["agent_rows"], d["agent_cols"], velocities=True)
+    cells = fs.inst[0].n_valid
+    del d
+    fs.step(3)  # warm-up (first launch, module load)
+    torch.cuda.synchronize(dev)
+    s0 = fs.controls()[0].step
+    t_couple, nbytes = 0.0, 0
+    t0 = time.perf_counter()
+    k = 1
+    while k * period <= sim_seconds + 1e-9:
+        fs.run_until(k * period, chunk=128)
+        c0 = time.perf_counter()
+        payload = msgpack.packb(be.gather())
+        t_couple += time.perf_counter() - c0
+        nbytes = len(payload)
+        k += 1
+    torch.cuda.synchronize(dev)
+    total = time.perf_counter() - t0
+    c = fs.controls()[0]
+    steps = c.step - s0
+    peak, peak_kind = measured_peak()
+    achieved = BYTES_PER_CELL_FP32 * cells * steps / total / 1e9
+    return {"value": cells * steps / total / 1e9, "unit": METRIC, "cells": cells,
+            "steps": steps, "sim_time_s": c.t, "wall_s": total, "agents": agents,
+            "couplings": k - 1, "coupling_s": t_couple,
+            "coupling_overhead": t_couple / total, "payload_bytes": nbytes,
+            "hbm_achieved_gbs": achieved, "hbm_frac": achieved / peak,
+            "peak_source": peak_kind,
+            "path": "FusedSolver.run_until (chunks of 128 launches, control-block read per "
+                    "chunk) + hb_gather of h, u, v + D2H + msgpack, wall clock"}
+
+
 def accuracy_vs_fp64(d: dict, dev, horizons=(64, 1000)) -> dict:
     """Max depth / velocity difference of the FP32 fused run against the FP64
     fused run at identical simulated times (the FP64 dt sequence replayed), and
@@ -528,6 +601,10 @@ def main() -> None:
     ap.add_argument("--no-ensemble", dest="ensemble", action="store_false")
     ap.add_argument("--ensemble-steps", type=int, default=20)
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false")
+    ap.add_argument("--no-coupled", dest="coupled", action="store_false")
+    ap.add_argument("--cpu-c1", action="store_true",
+                    help="also time the 256^2 dam break on the host (1 and all threads)")
+    ap.add_argument("--coupled-cells", type=int, default=8192)
     ap.add_argument("--adjoint-cells", type=int, default=1024)
     ap.add_argument("--adjoint-steps", type=int, default=2000)
     args = ap.parse_args()

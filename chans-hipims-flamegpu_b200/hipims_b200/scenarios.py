@@ -16,6 +16,11 @@ the shapes, sizes and value ranges of the workload it stands for.
                    16 Voronoi Manning zones from seeded sites with n drawn
                    from U(0.02, 0.10), 32 gauges on random valid cells,
                    rain 50 mm/h, optional initial pond
+  coupled_case     n x n (8192 in the headline case), 1 m cells, DEM as
+                   urban_catchment, rain 100 mm/h for 1800 s, Q_GIVEN inflow on
+                   the west edge (hydrograph 0 -> 500 -> 0 m^3/s over 1800 s as
+                   unit discharge sampled every 10 s), open elsewhere, and
+                   agent cells drawn uniformly over non-building cells
   channel          the 25 x 225 back-channel case: H_GIVEN inflow, OPEN
                    outflow, walls (HP/backCase.ipynb scenario, own geometry)
 
@@ -102,7 +107,7 @@ def urban_catchment(n: int = 2048, dx: float = 2.0, seed: int = 0, rain_mm_h: fl
     nodata = _ring(n, n)
     mask = boundary_codes(nodata, default_bc=50)
     z = np.zeros(mask.shape)
-    zi, _ = urban_dem(n, n, seed)
+    zi, bmask = urban_dem(n, n, seed)
     z[1:-1, 1:-1] = zi
     zone = np.ones(mask.shape, dtype=np.uint8)
     zone[1:-1, 1:-1] = np.where(road_mask(n, n, seed), 0, 1)
@@ -110,7 +115,8 @@ def urban_catchment(n: int = 2048, dx: float = 2.0, seed: int = 0, rain_mm_h: fl
     rate = rain_mm_h * MM_PER_H
     return dict(mask=mask, z=z, h=zeros.copy(), qx=zeros.copy(), qy=zeros.copy(), wl=z.copy(),
                 landuse=zone, manning=[0.035, 0.08], dx=dx, cfl=0.5, first_dt=1.0e-4,
-                rain=np.array([[0.0, rate], [duration, rate]]), t_end=duration)
+                rain=np.array([[0.0, rate], [duration, rate]]), t_end=duration,
+                buildings=bmask)
 
 
 def double_triangle_hyetograph(seed: int, duration: float = 3600.0) -> np.ndarray:
@@ -202,4 +208,25 @@ def adjoint_case(n: int = 1024, dx: float = 2.0, seed: int = 0, n_zones: int = 1
     rr, cc = np.nonzero(valid)
     pick = rng.choice(rr.size, size=n_gauges, replace=False)
     d["gauge_rows"], d["gauge_cols"] = rr[pick], cc[pick]
+    return d
+
+
+def coupled_case(n: int = 8192, dx: float = 1.0, seed: int = 0, agents: int = 100_000,
+                 peak_q: float = 500.0, duration: float = 1800.0) -> dict:
+    """Coupled-run rasters: urban DEM, 100 mm/h rain, a Q_GIVEN inflow edge
+    (west) with a triangular hydrograph peaking at peak_q m^3/s at duration/2,
+    given as unit discharge q = Q / (n dx) every 10 s, and `agents` agent cells
+    (row-major order, as the reference reports them) on non-building cells."""
+    d = urban_catchment(n, dx=dx, seed=seed, rain_mm_h=100.0, duration=duration)
+    nodata = _ring(n, n)
+    d["mask"] = boundary_codes(nodata, default_bc=50, boxes=[(1, n + 1, 1, 2, 7)])
+    t = np.arange(0.0, duration + 10.0, 10.0)
+    Q = peak_q * np.clip(1.0 - np.abs(t - duration / 2) / (duration / 2), 0.0, None)
+    d["given_q"] = np.stack([t, Q / (n * dx), np.zeros_like(t)], axis=1)
+    ok = np.zeros(d["mask"].shape, dtype=bool)
+    ok[1:-1, 1:-1] = ~d["buildings"]
+    rr, cc = np.nonzero(ok)
+    rng = np.random.default_rng(seed + 65537)
+    pick = np.sort(rng.choice(rr.size, size=min(agents, rr.size), replace=False))
+    d["agent_rows"], d["agent_cols"] = rr[pick], cc[pick]
     return d
