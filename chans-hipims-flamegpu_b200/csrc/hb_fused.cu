@@ -276,46 +276,18 @@ __device__ void bc_values_exact(const hb_instance &in, double t, BcTable *out) {
 // next export time, t += dt, FP64 volume / outflow / rain totals, and the rain
 // rate and boundary values of the next step.  Called by every thread of the
 // CTA that finished the instance's last tile.
+// The clock after a step: dt of the next step from the largest wave speed SM
+// and the any-dry flag D (HC/timeControl_Kernel.cu:164-198 per cell, torch.min,
+// then HP/SWE_CUDA.py:818-831: 10x cap, export clip, t += dt), the rain rate
+// and the boundary values at the new t.  All threads of the block call it;
+// thread 0 owns the control block.
 template <typename T, int NT>
-__device__ void finalize_instance(const hb_instance &in, int ii, TilePartial *partials,
-                                  BcTable *bct, double (*red_d)[NT / 32], double *red_s,
-                                  int *red_i) {
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+__device__ void advance_clock(const hb_instance &in, int ii, BcTable *bct, double SM, int D) {
+  const int tid = threadIdx.x;
   hb_ctrl *ctrl = in.ctrl;
-  __threadfence();
-  const int nt = in.tiles_x * in.tiles_y;
-  double v = 0, o = 0, sm = 0;
-  int dry = 0;
-  for (int k = tid; k < nt; k += NT) {
-    const TilePartial *pp = partials + in.tile_begin + k;
-    v += __ldcg(&pp->volume);
-    o += __ldcg(&pp->outflow);
-    sm = fmax(sm, __ldcg(&pp->smax));
-    dry |= __ldcg(&pp->any_dry);
-  }
-  v = warp_sum(v);
-  o = warp_sum(o);
-  sm = warp_max(sm);
-  dry = __any_sync(0xffffffffu, dry);
-  if (lane == 0) {
-    red_d[0][wid] = v;
-    red_d[1][wid] = o;
-    red_s[wid] = sm;
-    red_i[wid] = dry;
-  }
-  __syncthreads();
   __shared__ double s_tnew;
-  __shared__ int s_halt;
   if (tid == 0) {
-    double V = 0, O = 0, SM = 0;
-    int D = 0;
-    for (int w = 0; w < NT / 32; w++) {
-      V += red_d[0][w];
-      O += red_d[1][w];
-      SM = fmax(SM, red_s[w]);
-      D |= red_i[w];
-    }
-    const double dtn = ctrl->dt, tn = ctrl->t, dxd = in.dx;
+    const double dtn = ctrl->dt, tn = ctrl->t;
     // min over cells of CFL*dx/speed; the division is monotone, so dividing
     // once by the largest speed gives the same value.
     double cand = INFINITY;
@@ -333,13 +305,9 @@ __device__ void finalize_instance(const hb_instance &in, int ii, TilePartial *pa
     }
     if (in.dt_replay && ctrl->step < in.n_replay) dtnew = in.dt_replay[ctrl->step];
     if (!isfinite(dtnew)) ctrl->status |= 1;
-    ctrl->volume = V * dxd * dxd;
-    ctrl->outflow_volume += O * dtn * dxd;
-    ctrl->rain_volume += ctrl->rain_rate * dtn * dxd * dxd * (double)in.n_valid;
     const double tnew = tn + dtnew;
     ctrl->dt = dtnew;
     ctrl->t = tnew;
-    ctrl->cur = 1 - ctrl->cur;
     ctrl->step += 1;
     if (tnew >= ctrl->t_end) ctrl->halted = 1;
     s_tnew = tnew;
@@ -375,8 +343,79 @@ __device__ void finalize_instance(const hb_instance &in, int ii, TilePartial *pa
   } else if (tid == 32) {
     ctrl->rain_rate = rain_rate_at(in, ctrl, tnew);
   }
+}
+
+// Last tile of an instance: reduce the per-tile partials (FP64 volume and
+// outflow, largest wave speed, any dry cell), account the step's volumes,
+// flip the state buffer and advance the clock -- or, with external_dt,
+// leave the clock to hb_fused_finish and publish the speed and dry flag.
+template <typename T, int NT>
+__device__ void finalize_instance(const hb_instance &in, int ii, TilePartial *partials,
+                                  BcTable *bct, double (*red_d)[NT / 32], double *red_s,
+                                  int *red_i) {
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  hb_ctrl *ctrl = in.ctrl;
+  __threadfence();
+  const int nt = in.tiles_x * in.tiles_y;
+  double v = 0, o = 0, sm = 0;
+  int dry = 0;
+  for (int k = tid; k < nt; k += NT) {
+    const TilePartial *pp = partials + in.tile_begin + k;
+    v += __ldcg(&pp->volume);
+    o += __ldcg(&pp->outflow);
+    sm = fmax(sm, __ldcg(&pp->smax));
+    dry |= __ldcg(&pp->any_dry);
+  }
+  v = warp_sum(v);
+  o = warp_sum(o);
+  sm = warp_max(sm);
+  dry = __any_sync(0xffffffffu, dry);
+  if (lane == 0) {
+    red_d[0][wid] = v;
+    red_d[1][wid] = o;
+    red_s[wid] = sm;
+    red_i[wid] = dry;
+  }
+  __syncthreads();
+  __shared__ double s_sm;
+  __shared__ int s_dry, s_ext;
+  if (tid == 0) {
+    double V = 0, O = 0, SM = 0;
+    int D = 0;
+    for (int w = 0; w < NT / 32; w++) {
+      V += red_d[0][w];
+      O += red_d[1][w];
+      SM = fmax(SM, red_s[w]);
+      D |= red_i[w];
+    }
+    const double dtn = ctrl->dt, dxd = in.dx;
+    ctrl->volume = V * dxd * dxd;
+    ctrl->outflow_volume += O * dtn * dxd;
+    ctrl->rain_volume += ctrl->rain_rate * dtn * dxd * dxd * (double)in.n_valid;
+    ctrl->cur = 1 - ctrl->cur;
+    s_ext = ctrl->external_dt;
+    if (s_ext) {
+      ctrl->ext[0] = SM;
+      ctrl->ext[1] = D ? 1.0 : 0.0;
+    }
+    s_sm = SM;
+    s_dry = D;
+  }
+  __syncthreads();
+  if (!s_ext) advance_clock<T, NT>(in, ii, bct, s_sm, s_dry);
   if (tid == 0) ctrl->tiles_done = 0u;
-  (void)s_halt;
+}
+
+// hb_fused_finish: one block per instance advances the clock from the
+// speed / dry flag reduced over all strips, ext = [n_instances][2].
+template <typename T>
+__global__ void __launch_bounds__(kNT)
+finish_kernel(const hb_instance *__restrict__ insts, BcTable *__restrict__ bct,
+              const double *__restrict__ ext) {
+  const hb_instance &in = insts[blockIdx.x];
+  if (in.ctrl->halted) return;
+  advance_clock<T, kNT>(in, blockIdx.x, bct, ext[2 * blockIdx.x],
+                        ext[2 * blockIdx.x + 1] != 0.0 ? 1 : 0);
 }
 
 // Workspace layout: [n_tiles] TilePartial, [n_instances] BcTable, then
@@ -1610,6 +1649,20 @@ int prepare_impl(const hb_fused_batch *b, cudaStream_t st, CUtensorMap *host_map
 
 extern "C" int hb_fused_prepare(const hb_fused_batch *b, void *stream) {
   return prepare_impl(b, as_stream(stream), nullptr);
+}
+
+extern "C" int hb_fused_finish(const hb_fused_batch *b, const double *ext, void *stream) {
+  if (!b || !b->instances || !b->workspace || b->n_instances <= 0 || !ext)
+    return set_error(HB_ERR_ARG, "hb_fused_finish: bad batch record or null ext");
+  BcTable *bct = reinterpret_cast<BcTable *>((char *)b->workspace + ws_partials_bytes(b->n_tiles));
+  auto st = as_stream(stream);
+  if (b->dtype == HB_F64)
+    finish_kernel<double><<<b->n_instances, kNT, 0, st>>>(b->instances, bct, ext);
+  else if (b->dtype == HB_F32)
+    finish_kernel<float><<<b->n_instances, kNT, 0, st>>>(b->instances, bct, ext);
+  else
+    return set_error(HB_ERR_ARG, "hb_fused_finish: bad dtype %d", b->dtype);
+  return check_launch("hb_fused_finish");
 }
 
 extern "C" int hb_fused_step(const hb_fused_batch *b, int nsteps, void *stream) {

@@ -43,6 +43,7 @@ class HbCtrl(ctypes.Structure):
         ("exports", c_i32), ("rain_index", c_i32), ("tiles_done", ctypes.c_uint32),
         ("status", c_i32),
         ("bc_vals", (ctypes.c_float * 4) * HB_MAX_CLASSES),
+        ("external_dt", c_i32), ("pad1", c_i32), ("ext", c_dbl * 2),
     ]
 
 
@@ -111,6 +112,7 @@ SIGNATURES = {
     "hb_fused_prepare": (_I, [_P, _P]),
     "hb_fused_step": (_I, [_P, _I, _P]),
     "hb_fused_step_noalloc": (_I, [_P, _I, _I, _P]),
+    "hb_fused_finish": (_I, [_P, _P, _P]),
     "hb_adjoint_step": (_I, [_P, _P]),
     "hb_adjoint_gauge": (_I, [_L, _P, _P, _P, _P, ctypes.c_double, _P]),
     "hb_gather": (_I, [_I, _L, _P, _P, _P, _P, _P, _P, _P, _P]),

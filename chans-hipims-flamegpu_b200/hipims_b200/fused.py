@@ -59,6 +59,17 @@ class Catchment:
     cum: np.ndarray | None = None           # initial cumulative infiltrated depth (m)
 
 
+def block_datum(valid: np.ndarray, z: np.ndarray, block: int = 64) -> np.ndarray:
+    """Integer bed datum of every block x block block: floor of the lowest
+    valid bed elevation in it (0 for a block without valid cells)."""
+    rows, cols = valid.shape
+    nby, nbx = (rows + block - 1) // block, (cols + block - 1) // block
+    zv = np.full((nby * block, nbx * block), np.inf)
+    zv[:rows, :cols] = np.where(valid, z, np.inf)
+    m = zv.reshape(nby, block, nbx, block).min(axis=(1, 3))
+    return np.where(np.isfinite(m), np.floor(np.where(np.isfinite(m), m, 0.0)), 0.0)
+
+
 def _round_up(x: int, m: int) -> int:
     return (x + m - 1) // m * m
 
@@ -104,14 +115,7 @@ class _Instance:
         z = np.asarray(c.z, dtype=np.float64)
         fp32 = dtype == torch.float32
         nby, nbx = (rows + 63) // 64, (cols + 63) // 64
-        datum = np.zeros((nby, nbx), dtype=np.float64)
-        if fp32:
-            zv = np.where(valid, z, np.inf)
-            for by in range(nby):
-                for bx in range(nbx):
-                    blk = zv[by * 64:(by + 1) * 64, bx * 64:(bx + 1) * 64]
-                    m = blk.min()
-                    datum[by, bx] = math.floor(m) if np.isfinite(m) else 0.0
+        datum = block_datum(valid, z) if fp32 else np.zeros((nby, nbx), dtype=np.float64)
         self.datum_np = datum
         dfull = np.repeat(np.repeat(datum, 64, axis=0), 64, axis=1)[:rows, :cols]
         zrel = np.where(valid, z - dfull, 0.0)
@@ -297,6 +301,17 @@ class FusedSolver:
         for z_ in range(_lib.HB_MAX_ZONES):
             self._recs_host[k].manning[z_] = vals[z_]
         self.records.copy_(torch.frombuffer(bytearray(self._recs_host), dtype=torch.uint8))
+
+    def set_external_dt(self, on: bool = True) -> None:
+        """Defer the clock of every instance to hb_fused_finish (strips of one
+        catchment: the next dt needs the wave speed of all strips)."""
+        n = len(self.inst)
+        init = (_lib.HbCtrl * n).from_buffer_copy(self._ctrl_init)
+        cs = self.controls()
+        for k in range(n):
+            init[k].external_dt = cs[k].external_dt = 1 if on else 0
+        self._ctrl_init = bytes(init)
+        self.write_controls(cs)
 
     def reset(self, rain_mult: Sequence[float] | float | None = None) -> None:
         """Back to the initial state and control blocks of the catchments

@@ -130,6 +130,14 @@ size_t hb_fused_workspace_size(const struct hb_fused_batch *batch);
 int hb_fused_prepare(const struct hb_fused_batch *batch, void *stream);
 /* Enqueue `nsteps` fused steps (graph-capturable; no host sync). */
 int hb_fused_step(const struct hb_fused_batch *batch, int nsteps, void *stream);
+/* Clock advance of instances stepped with hb_ctrl.external_dt set (no
+ * counterpart in the reference; one catchment split into row strips over
+ * several instances or GPUs): ext = device [n_instances][2], the largest wave
+ * speed and the any-dry flag of each instance's whole catchment (the maximum
+ * of hb_ctrl.ext over its strips).  Applies HP/SWE_CUDA.py:818-831 (CFL dt,
+ * 10x cap, export clip, t += dt) and sets the next step's rain rate and
+ * boundary values.  One step, then this, per time step. */
+int hb_fused_finish(const struct hb_fused_batch *batch, const double *ext, void *stream);
 
 /* Allocation-free variant of hb_fused_step (no counterpart in the reference).
  * For callers that must not allocate device memory: host programs that own a

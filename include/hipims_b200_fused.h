@@ -68,6 +68,15 @@ typedef struct hb_ctrl {
   uint32_t tiles_done;   /* internal last-tile-done counter */
   int32_t status;        /* nonzero: a NaN/inf was seen in dt */
   float bc_vals[HB_MAX_CLASSES][4]; /* given h, wl, qx, qy per class at t */
+  /* Deferred time step (strips of one catchment on several instances or
+   * GPUs): with external_dt set, a step leaves dt, t, the step counter and
+   * the next step's rain rate and boundary values alone and writes its
+   * largest wave speed and whether any valid cell was dry to ext[0], ext[1];
+   * hb_fused_finish then advances the clock from values reduced over all
+   * strips (max of each). */
+  int32_t external_dt;
+  int32_t pad1;
+  double ext[2];
 } hb_ctrl;
 
 /* One catchment.  Pointers are device pointers. */
