@@ -205,14 +205,37 @@ def run_ours(args) -> None:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    d = workload(args.cells)
-    fs = FusedSolver(catchment_from(d), dtype=torch.float32, tile=tuple(args.tile), device=dev,
-                     minb=args.minb)
-    n_valid = fs.inst[0].n_valid
+    strips = None
+    if args.strips:
+        # one catchment of (ranks x n) x n cells split in row strips, one per
+        # rank (weak scaling with a halo exchange and a clock all_reduce per
+        # step); on one GPU, the n x n catchment in two strips of one batch
+        from hipims_b200 import scenarios as S
+        from hipims_b200.strips import DistributedStrips, StripSolver
+
+        d = S.urban_catchment(args.cells, dx=2.0, seed=0, n_rows=args.cells * max(world, 1))
+        if world > 1:
+            strips = DistributedStrips(catchment_from(d), rank, world, dtype=torch.float32,
+                                       tile=tuple(args.tile), device=dev, minb=args.minb)
+        else:
+            strips = StripSolver(catchment_from(d), 2, dtype=torch.float32,
+                                 tile=tuple(args.tile), device=dev, minb=args.minb)
+        fs = strips.fs
+    else:
+        d = workload(args.cells)
+        fs = FusedSolver(catchment_from(d), dtype=torch.float32, tile=tuple(args.tile),
+                         device=dev, minb=args.minb)
+    n_valid = sum(i.n_valid for i in fs.inst)  # this rank's cells
+    total_cells = n_valid
+    if world > 1:
+        tc = torch.tensor([float(n_valid)], device=dev, dtype=torch.float64)
+        dist.all_reduce(tc)
+        total_cells = int(tc.item())
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stepper = strips if strips is not None else fs
 
-    fs.step(SPINUP + args.warmup)
+    stepper.step(SPINUP + args.warmup)
     torch.cuda.synchronize(dev)
 
     def barrier():
@@ -228,7 +251,7 @@ def run_ours(args) -> None:
     for a, b in ev:
         flush.fill_(1)
         a.record(stream)
-        fs.step(1)
+        stepper.step(1)
         b.record(stream)
     barrier()
     clk = clocks.stop()
@@ -238,16 +261,15 @@ def run_ours(args) -> None:
         t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-    value = world * n_valid * args.steps / (total_ms * 1e-3) / 1e9
+    value = total_cells * args.steps / (total_ms * 1e-3) / 1e9
     c = fs.controls()[0]
 
     # end to end through the C ABI with host buffers: H2D of the state from
     # pinned memory, one fused step, D2H of the new state, every step
-    ins = fs.inst[0]
-    host_in = [torch.empty_like(x, device="cpu").pin_memory() for x in (ins.h[0], ins.qx[0],
-                                                                        ins.qy[0])]
+    state = lambda b: [x for ins in fs.inst for x in (ins.h[b], ins.qx[b], ins.qy[b])]
+    host_in = [torch.empty_like(x, device="cpu").pin_memory() for x in state(0)]
     host_out = [torch.empty_like(x) for x in host_in]
-    for hsrc, x in zip(host_in, (ins.h[c.cur], ins.qx[c.cur], ins.qy[c.cur])):
+    for hsrc, x in zip(host_in, state(c.cur)):
         hsrc.copy_(x)
     cur = c.cur
     e2e_steps = min(args.steps, 200)
@@ -255,11 +277,11 @@ def run_ours(args) -> None:
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(e2e_steps):
-        for hsrc, x in zip(host_in, (ins.h[cur], ins.qx[cur], ins.qy[cur])):
+        for hsrc, x in zip(host_in, state(cur)):
             x.copy_(hsrc, non_blocking=True)
-        fs.step(1)
+        stepper.step(1)
         cur = 1 - cur
-        for hdst, x in zip(host_out, (ins.h[cur], ins.qx[cur], ins.qy[cur])):
+        for hdst, x in zip(host_out, state(cur)):
             hdst.copy_(x, non_blocking=True)
     e1.record(stream)
     barrier()
@@ -268,7 +290,7 @@ def run_ours(args) -> None:
         t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    e2e = world * n_valid * e2e_steps / (e2e_ms * 1e-3) / 1e9
+    e2e = total_cells * e2e_steps / (e2e_ms * 1e-3) / 1e9
     bytes_io = sum(x.numel() * x.element_size() for x in host_in)
 
     if rank == 0:
@@ -283,7 +305,8 @@ def run_ours(args) -> None:
             "data": "synthetic", "impl": "ours",
             "config": config_of(args.cells, world, {"tile": list(args.tile),
                                                      "min_blocks_per_sm": args.minb,
-                                                     "sim_time_s": c.t, "dt_s": c.dt}),
+                                                     "sim_time_s": c.t, "dt_s": c.dt,
+                                                     **strip_config(args, world)}),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "kernel": f"rows_step_kernel<float,{args.tile[0]},minb={args.minb}>",
@@ -293,11 +316,11 @@ def run_ours(args) -> None:
                     "d2h_bytes_per_step": bytes_io, "steps": e2e_steps,
                     "path": "pinned host h, qx, qy -> device; hb_fused_step; device -> "
                             "pinned host, every step"},
-            "gpu_launches": args.steps,
+            "gpu_launches": args.steps * (2 if strips is not None else 1),
             "clocks": clk,
             "step_ms_min": min(step_ms), "step_ms_max": max(step_ms),
         }
-        if args.accuracy:
+        if args.accuracy and world == 1 and not args.strips:
             line["accuracy"] = accuracy_vs_fp64(d, dev)
         if args.plain and world == 1:
             pl = plain_fp64_rate(d, dev, reference_kernels=True)
@@ -328,6 +351,18 @@ def run_ours(args) -> None:
         dist.barrier()
         dist.destroy_process_group()
     del _lib
+
+
+def strip_config(args, world: int) -> dict:
+    if not args.strips:
+        return {}
+    if world > 1:
+        return {"decomposition": f"one {args.cells * world}x{args.cells} catchment in {world} "
+                                 f"row strips, one per GPU: NCCL halo exchange (2 rows of h, "
+                                 f"qx, qy each way) and all_reduce(MAX) of the clock inputs "
+                                 f"per step", "parallelism": f"strips x{world}"}
+    return {"decomposition": f"one {args.cells}x{args.cells} catchment in 2 row strips on one "
+                             f"GPU (device halo copies, clock reduced by torch max)"}
 
 
 def plain_fp64_rate(d: dict, dev, steps: int = 5, reference_kernels: bool = True) -> dict:
@@ -602,6 +637,9 @@ def main() -> None:
     ap.add_argument("--ensemble-steps", type=int, default=20)
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false")
     ap.add_argument("--no-coupled", dest="coupled", action="store_false")
+    ap.add_argument("--strips", action="store_true",
+                    help="one catchment split in row strips over the GPUs (halo exchange) "
+                         "instead of independent replicas")
     ap.add_argument("--cpu-c1", action="store_true",
                     help="also time the 256^2 dam break on the host (1 and all threads)")
     ap.add_argument("--coupled-cells", type=int, default=8192)

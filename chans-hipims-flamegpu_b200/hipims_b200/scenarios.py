@@ -102,15 +102,17 @@ def dam_break(n: int = 256, ring_code: int = 40, manning: float = 0.03) -> dict:
 
 
 def urban_catchment(n: int = 2048, dx: float = 2.0, seed: int = 0, rain_mm_h: float = 50.0,
-                    duration: float = 3600.0) -> dict:
-    """Config 2 rasters and settings (single instance)."""
-    nodata = _ring(n, n)
+                    duration: float = 3600.0, n_rows: int | None = None) -> dict:
+    """Config 2 rasters and settings (single instance); n_rows x n valid cells
+    when n_rows is given (default square)."""
+    m = n if n_rows is None else n_rows
+    nodata = _ring(m, n)
     mask = boundary_codes(nodata, default_bc=50)
     z = np.zeros(mask.shape)
-    zi, bmask = urban_dem(n, n, seed)
+    zi, bmask = urban_dem(m, n, seed)
     z[1:-1, 1:-1] = zi
     zone = np.ones(mask.shape, dtype=np.uint8)
-    zone[1:-1, 1:-1] = np.where(road_mask(n, n, seed), 0, 1)
+    zone[1:-1, 1:-1] = np.where(road_mask(m, n, seed), 0, 1)
     zeros = np.zeros(mask.shape)
     rate = rain_mm_h * MM_PER_H
     return dict(mask=mask, z=z, h=zeros.copy(), qx=zeros.copy(), qy=zeros.copy(), wl=z.copy(),
