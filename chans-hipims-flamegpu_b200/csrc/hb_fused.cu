@@ -213,6 +213,24 @@ __device__ double rain_rate_at(const hb_instance &in, hb_ctrl *c, double t) {
   return (r0[1] + per * (r1[1] - r0[1])) * c->rain_mult;
 }
 
+// Rates of every rain station at t (HP/SWE_CUDA.py:472-502: the row cursor
+// rain_rate_at left in the control block, linear interpolation per station
+// column, zero from the last row on), stations first, first + stride, ...
+__device__ void station_rates_at(const hb_instance &in, const hb_ctrl *c, double t, int first,
+                                 int stride) {
+  if (!in.rain_station) return;
+  const double *R = in.rain_tab;
+  const int C = in.rain_cols;
+  const bool inside = R && in.rain_rows >= 2 && t < R[(int64_t)(in.rain_rows - 1) * C];
+  const double *r0 = inside ? R + (int64_t)c->rain_index * C : nullptr;
+  const double per = inside ? (t - r0[0]) / (r0[C] - r0[0]) : 0.0;
+  for (int k = first; k < in.n_stations; k += stride) {
+    double rate = 0.0;
+    if (inside && k + 1 < C) rate = (r0[k + 1] + per * (r0[C + k + 1] - r0[k + 1])) * c->rain_mult;
+    in.station_rate[k] = rate;
+  }
+}
+
 // Boundary values of every class at t (step-function lookup,
 // HC/flucCal_2ndOrder_jh_improved_Kernel.cu:355-366, 441-446).
 __device__ void bc_values_at(const hb_instance &in, hb_ctrl *c, double t) {
@@ -343,6 +361,10 @@ __device__ void advance_clock(const hb_instance &in, int ii, BcTable *bct, doubl
   } else if (tid == 32) {
     ctrl->rain_rate = rain_rate_at(in, ctrl, tnew);
   }
+  if (in.rain_station) {
+    __syncthreads();  // the rain cursor
+    station_rates_at(in, ctrl, tnew, tid, NT);
+  }
 }
 
 // Last tile of an instance: reduce the per-tile partials (FP64 volume and
@@ -391,7 +413,13 @@ __device__ void finalize_instance(const hb_instance &in, int ii, TilePartial *pa
     const double dtn = ctrl->dt, dxd = in.dx;
     ctrl->volume = V * dxd * dxd;
     ctrl->outflow_volume += O * dtn * dxd;
-    ctrl->rain_volume += ctrl->rain_rate * dtn * dxd * dxd * (double)in.n_valid;
+    if (in.rain_station) {
+      double rv = 0.0;
+      for (int k = 0; k < in.n_stations; k++) rv += in.station_rate[k] * in.station_cells[k];
+      ctrl->rain_volume += rv * dtn * dxd * dxd;
+    } else {
+      ctrl->rain_volume += ctrl->rain_rate * dtn * dxd * dxd * (double)in.n_valid;
+    }
     ctrl->cur = 1 - ctrl->cur;
     s_ext = ctrl->external_dt;
     if (s_ext) {
@@ -1178,6 +1206,7 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
     const int rx = x0 + j;
     // read once per tile: the state stores below may alias the record
     const bool infil = in.cum != nullptr;
+    const bool stations = in.rain_station != nullptr;
 
 #pragma unroll 1
     for (int i = r0; i < r0 + R; ++i) {
@@ -1257,7 +1286,13 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
             outf += o;
           }
         }
-        hu += rain * dt;
+        if (stations) {
+          // station rain (HC/stationPrecipitation_Kernel.cu:18-29), every valid cell
+          const size_t gs = (size_t)(ry + HB_PAD_Y) * P + (rx + HB_PAD_X);
+          hu += (T)in.station_rate[in.rain_station[gs]] * dt;
+        } else {
+          hu += rain * dt;
+        }
         if (infil && active) {
           // Green-Ampt infiltration on the flux list, after rain
           // (HC/infiltrationCUDA_Kernel.cu:20-46; order HP/CatchFlood_main.py:164-170)
@@ -1414,6 +1449,10 @@ prepare_kernel(const hb_instance *__restrict__ insts, BcTable *__restrict__ bct)
     c->rain_rate = rain_rate_at(in, c, c->t);
     bc_values_exact(in, c->t, &bct[blockIdx.x]);
     bc_values_at(in, c, c->t);
+  }
+  if (in.rain_station) {
+    __syncthreads();  // the rain cursor
+    station_rates_at(in, c, c->t, threadIdx.x, blockDim.x);
   }
 }
 
@@ -1618,8 +1657,9 @@ int prepare_impl(const hb_fused_batch *b, cudaStream_t st, CUtensorMap *host_map
   }
   if (!uses_rows_kernel(b) && b->instances_host) {
     for (int i = 0; i < b->n_instances; i++)
-      if (b->instances_host[i].cum)
-        return set_error(HB_ERR_ARG, "hb_fused_prepare: infiltration needs the rows kernel");
+      if (b->instances_host[i].cum || b->instances_host[i].rain_station)
+        return set_error(HB_ERR_ARG,
+                         "hb_fused_prepare: infiltration and station rain need the rows kernel");
   }
   BcTable *bct = reinterpret_cast<BcTable *>((char *)b->workspace + ws_partials_bytes(b->n_tiles));
   // blocks per instance for the volume sum: about 16 cells per thread of the

@@ -65,6 +65,8 @@ class HbInstance(ctypes.Structure):
         ("dt_replay", c_vp), ("n_replay", c_i64),
         ("cum", c_vp), ("ks", c_dbl * HB_MAX_ZONES), ("psi", c_dbl * HB_MAX_ZONES),
         ("dtheta", c_dbl * HB_MAX_ZONES),
+        ("rain_station", c_vp), ("station_rate", c_vp), ("station_cells", c_vp),
+        ("n_stations", c_i32), ("pad2", c_i32),
     ]
 
 

@@ -82,8 +82,8 @@ class GaugeMisfit:
             raise ValueError(f"dt schedule has {dts.shape[0]} steps, {nsteps} needed")
         if every < 1 or checkpoint < 1:
             raise ValueError("every and checkpoint must be >= 1")
-        if catchment.infiltration is not None:
-            raise ValueError("the adjoint does not include infiltration")
+        if catchment.infiltration is not None or catchment.rain_station is not None:
+            raise ValueError("the adjoint covers uniform rain without infiltration")
         self.catchment = dataclasses.replace(
             catchment, dt0=float(dts[0]), dt_replay=dts[1:nsteps].copy() if nsteps > 1 else
             np.zeros(1), export_step=0.0, t_end=math.inf, halt_on_export=False)

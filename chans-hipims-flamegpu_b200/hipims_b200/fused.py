@@ -57,6 +57,9 @@ class Catchment:
     # Green-Ampt infiltration: {"ks", "psi", "dtheta"} per Manning zone (m/s, m, -)
     infiltration: dict | None = None
     cum: np.ndarray | None = None           # initial cumulative infiltrated depth (m)
+    # station rain: station id of every cell (raster); rain is then [T, 1 + S]
+    # with one rate column per station (HP/SWE_CUDA.py:472-502)
+    rain_station: np.ndarray | None = None
 
 
 def block_datum(valid: np.ndarray, z: np.ndarray, block: int = 64) -> np.ndarray:
@@ -152,6 +155,18 @@ class _Instance:
         self.rain = None if c.rain is None else table(c.rain, 2)
         self.dt_replay = None if c.dt_replay is None else torch.as_tensor(
             np.asarray(c.dt_replay, dtype=np.float64), device=device).contiguous()
+        self.rain_station = None
+        if c.rain_station is not None:
+            st = np.where(valid, np.asarray(c.rain_station), 0).astype(np.int64)
+            n_st = (self.rain.shape[1] - 1) if self.rain is not None else 0
+            if n_st < 1 or st.min(initial=0) < 0 or st.max(initial=0) >= n_st:
+                raise ValueError("rain_station ids must index the rain table's station columns")
+            dense_st = np.zeros((rows_s, pitch), dtype=np.int16)
+            dense_st[PY:PY + rows, PX:PX + cols] = st.astype(np.int16)
+            self.rain_station = torch.as_tensor(dense_st, device=device).contiguous()
+            self.station_cells = torch.as_tensor(
+                np.bincount(st[valid], minlength=n_st).astype(np.float64), device=device)
+            self.station_rate = torch.zeros(n_st, dtype=torch.float64, device=device)
         self.cum = None
         self.infil = None
         if c.infiltration is not None:
@@ -250,6 +265,13 @@ class FusedSolver:
             if ins.dt_replay is not None:
                 r.dt_replay = ins.dt_replay.data_ptr()
                 r.n_replay = ins.dt_replay.numel()
+            if ins.rain_station is not None:
+                if kernel == "tasks":
+                    raise ValueError("station rain needs the rows kernel")
+                r.rain_station = ins.rain_station.data_ptr()
+                r.station_rate = ins.station_rate.data_ptr()
+                r.station_cells = ins.station_cells.data_ptr()
+                r.n_stations = ins.station_rate.numel()
             if ins.cum is not None:
                 if kernel == "tasks":
                     raise ValueError("infiltration needs the rows kernel")

@@ -60,7 +60,7 @@ def strip_catchment(c: Catchment, a: int, b: int) -> Catchment:
     cut = lambda x: None if x is None else np.asarray(x)[a:b]
     return dataclasses.replace(
         c, mask=cut(c.mask), z=cut(c.z), h=cut(c.h), qx=cut(c.qx), qy=cut(c.qy),
-        zone=cut(c.zone), h_max=cut(c.h_max), cum=cut(c.cum))
+        zone=cut(c.zone), h_max=cut(c.h_max), cum=cut(c.cum), rain_station=cut(c.rain_station))
 
 
 def _first_valid(mask: np.ndarray) -> tuple[int, int]:

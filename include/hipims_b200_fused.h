@@ -115,6 +115,15 @@ typedef struct hb_instance {
   double ks[HB_MAX_ZONES];   /* saturated hydraulic conductivity per zone (m/s) */
   double psi[HB_MAX_ZONES];  /* capillary head per zone (m) */
   double dtheta[HB_MAX_ZONES]; /* water-content difference per zone */
+  /* optional station rain (HC/stationPrecipitation_Kernel.cu:18-29 with the
+   * station interpolation of HP/SWE_CUDA.py:472-502): rain_tab holds one rate
+   * column per station, rain_station the station of every cell (dense like h);
+   * NULL rain_station: uniform rain from column 1.  Rows kernel only. */
+  const uint16_t *rain_station;
+  double *station_rate;      /* [n_stations] rates at t, kept by the library */
+  const double *station_cells; /* [n_stations] valid cells per station */
+  int32_t n_stations;
+  int32_t pad2;
 } hb_instance;
 
 /* Launch record (host memory). */
