@@ -1047,7 +1047,7 @@ __device__ __forceinline__ FaceOut<T> face_any(const RowsSmem<T, TY> &s, const C
   return o;
 }
 
-template <typename T, int TY, bool FAST, int MINB>
+template <typename T, int TY, bool FAST, int MINB, bool SOURCES = false>
 __global__ void __launch_bounds__(kRowsNT, MINB)
 rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restrict__ tile_inst,
                  int n_tiles, TilePartial *__restrict__ partials, BcTable *__restrict__ bct,
@@ -1205,8 +1205,10 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
     T *hmaxg = (T *)in.h_max;
     const int rx = x0 + j;
     // read once per tile: the state stores below may alias the record
-    const bool infil = in.cum != nullptr;
-    const bool stations = in.rain_station != nullptr;
+    // (instances without infiltration or station rain take the SOURCES = false
+    // build, in which both branches vanish)
+    const bool infil = SOURCES && in.cum != nullptr;
+    const bool stations = SOURCES && in.rain_station != nullptr;
 
 #pragma unroll 1
     for (int i = r0; i < r0 + R; ++i) {
@@ -1518,18 +1520,18 @@ int launch_steps(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   return check_launch("hb_fused_step");
 }
 
-template <typename T, int TY, bool FAST = (sizeof(T) == 4), int MINB = 1>
-int launch_rows(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
+template <typename T, int TY, bool FAST = (sizeof(T) == 4), int MINB = 1, bool SOURCES = false>
+int launch_rows_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   using S = RowsSmem<T, TY>;
   static std::once_flag once;
   static cudaError_t attr_err = cudaSuccess;
   static int blocks_per_sm = 1;
   std::call_once(once, [] {
-    attr_err = cudaFuncSetAttribute(rows_step_kernel<T, TY, FAST, MINB>,
+    attr_err = cudaFuncSetAttribute(rows_step_kernel<T, TY, FAST, MINB, SOURCES>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(S));
     if (attr_err == cudaSuccess)
       attr_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &blocks_per_sm, rows_step_kernel<T, TY, FAST, MINB>, kRowsNT, sizeof(S));
+          &blocks_per_sm, rows_step_kernel<T, TY, FAST, MINB, SOURCES>, kRowsNT, sizeof(S));
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   });
   if (attr_err != cudaSuccess)
@@ -1541,10 +1543,18 @@ int launch_rows(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   BcTable *bct = reinterpret_cast<BcTable *>(ws + ws_partials_bytes(b->n_tiles));
   const CUtensorMap *maps = reinterpret_cast<const CUtensorMap *>(ws + ws_maps_offset(b));
   for (int k = 0; k < nsteps; k++) {
-    rows_step_kernel<T, TY, FAST, MINB><<<grid, kRowsNT, sizeof(S), st>>>(
+    rows_step_kernel<T, TY, FAST, MINB, SOURCES><<<grid, kRowsNT, sizeof(S), st>>>(
         b->instances, b->tile_instance, b->n_tiles, parts, bct, maps);
   }
   return check_launch("hb_fused_step");
+}
+
+// The build with the infiltration / station-rain branches when the batch
+// says its instances use them (HB_FLAG_SOURCES).
+template <typename T, int TY, bool FAST = (sizeof(T) == 4), int MINB = 1>
+int launch_rows(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
+  if (b->flags & HB_FLAG_SOURCES) return launch_rows_impl<T, TY, FAST, MINB, true>(b, nsteps, st);
+  return launch_rows_impl<T, TY, FAST, MINB, false>(b, nsteps, st);
 }
 
 bool uses_rows_kernel(const hb_fused_batch *b) { return !(b->flags & HB_FLAG_TILE_TASKS); }
@@ -1655,11 +1665,16 @@ int prepare_impl(const hb_fused_batch *b, cudaStream_t st, CUtensorMap *host_map
     }
     if (rc) return rc;
   }
-  if (!uses_rows_kernel(b) && b->instances_host) {
-    for (int i = 0; i < b->n_instances; i++)
-      if (b->instances_host[i].cum || b->instances_host[i].rain_station)
+  if (b->instances_host) {
+    for (int i = 0; i < b->n_instances; i++) {
+      const bool src = b->instances_host[i].cum || b->instances_host[i].rain_station;
+      if (src && !uses_rows_kernel(b))
         return set_error(HB_ERR_ARG,
                          "hb_fused_prepare: infiltration and station rain need the rows kernel");
+      if (src && !(b->flags & HB_FLAG_SOURCES))
+        return set_error(HB_ERR_ARG, "hb_fused_prepare: instance %d has infiltration or "
+                                     "station rain; set HB_FLAG_SOURCES", i);
+    }
   }
   BcTable *bct = reinterpret_cast<BcTable *>((char *)b->workspace + ws_partials_bytes(b->n_tiles));
   // blocks per instance for the volume sum: about 16 cells per thread of the

@@ -296,7 +296,9 @@ class FusedSolver:
         b.tile_y, b.tile_x = self.tile
         b.grid_blocks = grid_blocks
         b.order = 2
-        b.flags = (1 if exact_fp32 else 0) | (2 if kernel == "tasks" else 0) | (minb << 8)
+        sources = any(i.cum is not None or i.rain_station is not None for i in self.inst)
+        b.flags = ((1 if exact_fp32 else 0) | (2 if kernel == "tasks" else 0) |
+                   (4 if sources else 0) | (minb << 8))
         b.instances_host = ctypes.addressof(self._recs_host)
         b.instances = self.records.data_ptr()
         b.tile_instance = self.tile_instance.data_ptr()

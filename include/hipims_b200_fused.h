@@ -40,6 +40,9 @@ extern "C" {
 /* hb_fused_batch.flags: use the face-task kernel (any 32x32 tile, staged by
  * plain loads) instead of the row-walking kernel (32-wide tiles staged by TMA). */
 #define HB_FLAG_TILE_TASKS 2
+/* hb_fused_batch.flags: some instance has infiltration or station rain (the
+ * rows kernel build with those source terms; hb_fused_prepare checks it). */
+#define HB_FLAG_SOURCES 4
 /* hb_fused_batch.flags bits 8-11: register cap of the rows kernel expressed
  * as resident CTAs per SM (0 = compiler default; 5, 6 for 32-row tiles; 4 for
  * 64-row tiles).  The autotuner picks it. */
