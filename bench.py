@@ -268,7 +268,7 @@ def run_ours(args) -> None:
     # pinned memory, one fused step, D2H of the new state, every step
     state = lambda b: [x for ins in fs.inst for x in (ins.h[b], ins.qx[b], ins.qy[b])]
     host_in = [torch.empty_like(x, device="cpu").pin_memory() for x in state(0)]
-    host_out = [torch.empty_like(x) for x in host_in]
+    host_out = [torch.empty_like(x).pin_memory() for x in host_in]
     for hsrc, x in zip(host_in, state(c.cur)):
         hsrc.copy_(x)
     cur = c.cur
