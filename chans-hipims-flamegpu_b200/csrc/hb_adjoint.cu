@@ -243,7 +243,7 @@ adj_cell_kernel(hb_adjoint_args a) {
 }
 
 // Pass 2: per face, owned by its east (x) / south (y) cell.
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(128)
 adj_face_kernel(hb_adjoint_args a) {
   __shared__ BcVals bc;
   const hb_instance &in = *a.instance;
@@ -305,8 +305,11 @@ extern "C" int hb_adjoint_step(const hb_adjoint_args *a, void *stream) {
   adj_cell_kernel<<<g1, blk, 0, st>>>(*a);
   int rc = check_launch("hb_adjoint_step (cells)");
   if (rc) return rc;
-  const dim3 g2((a->cols + 1 + 31) / 32, (a->rows + 1 + 7) / 8);
-  adj_face_kernel<<<g2, blk, 0, st>>>(*a);
+  // 128-thread blocks: the face pass needs ~156 registers a thread, so three
+  // blocks (12 warps) fit an SM where one 256-thread block would
+  const dim3 blk2(32, 4);
+  const dim3 g2((a->cols + 1 + 31) / 32, (a->rows + 1 + 3) / 4);
+  adj_face_kernel<<<g2, blk2, 0, st>>>(*a);
   return check_launch("hb_adjoint_step (faces)");
 }
 
