@@ -411,6 +411,7 @@ __device__ void finalize_instance(const hb_instance &in, int ii, TilePartial *pa
       D |= red_i[w];
     }
     const double dtn = ctrl->dt, dxd = in.dx;
+    if (!isfinite(V)) ctrl->status |= 4;  // a NaN / inf depth somewhere in the raster
     ctrl->volume = V * dxd * dxd;
     ctrl->outflow_volume += O * dtn * dxd;
     if (in.rain_station) {

@@ -414,6 +414,19 @@ class FusedSolver:
         arr = (_lib.HbCtrl * n)(*ctrls)
         self.ctrl.copy_(torch.frombuffer(bytearray(arr), dtype=torch.uint8))
 
+    STATUS = {1: "non-finite time step", 2: "a tile's data did not arrive in time",
+              4: "non-finite depth"}
+
+    def check(self) -> None:
+        """Raise if a step flagged a failure in any control block (syncs)."""
+        bad = []
+        for k, c in enumerate(self.controls()):
+            if c.status:
+                why = ", ".join(m for b, m in self.STATUS.items() if c.status & b)
+                bad.append(f"instance {k} at t = {c.t:.6g} s, step {c.step}: {why}")
+        if bad:
+            raise FloatingPointError("fused step failed: " + "; ".join(bad))
+
     def resume(self, k: int | None = None) -> None:
         """Clear the halted flag (after an export halt) of one or all instances."""
         cs = self.controls()
@@ -433,6 +446,8 @@ class FusedSolver:
         while True:
             self.step(chunk)
             cs = self.controls()
+            if any(c.status for c in cs):
+                self.check()
             steps = max(c.step for c in cs) - start
             if all(c.halted for c in cs) or steps >= max_steps:
                 return steps

@@ -69,7 +69,8 @@ typedef struct hb_ctrl {
   int32_t exports;       /* export clips taken */
   int32_t rain_index;    /* monotone cursor into the rain table */
   uint32_t tiles_done;   /* internal last-tile-done counter */
-  int32_t status;        /* nonzero: a NaN/inf was seen in dt */
+  int32_t status;        /* bits: 1 non-finite dt, 2 a tile's data did not arrive
+                            (TMA wait timed out), 4 non-finite depth (FP64 volume) */
   float bc_vals[HB_MAX_CLASSES][4]; /* given h, wl, qx, qy per class at t */
   /* Deferred time step (strips of one catchment on several instances or
    * GPUs): with external_dt set, a step leaves dt, t, the step counter and

@@ -357,3 +357,23 @@ def test_fused_station_rain_matches_oracle(cuda, dtype, tol):
     assert c.rain_volume > 0
     bal = abs(c.volume - c.volume0 - c.rain_volume + c.outflow_volume) / c.rain_volume
     assert bal < (1e-9 if dtype == torch.float64 else 1e-4)
+
+
+def test_non_finite_state_is_reported(cuda):
+    """A NaN depth (a blown-up run) sets the control block's status and the
+    host raises at the next check; a healthy run reports nothing."""
+    from hipims_b200 import scenarios as S
+    from hipims_b200.fused import FusedSolver
+
+    d = S.dam_break(48)
+    fs = FusedSolver(catchment(d), dtype=torch.float32, device=cuda)
+    fs.step(5)
+    fs.check()
+    h = fs.current()[0]
+    h[10, 10] = float("nan")
+    fs.step(1)
+    assert fs.controls()[0].status & 4
+    with pytest.raises(FloatingPointError, match="non-finite depth"):
+        fs.check()
+    with pytest.raises(FloatingPointError):
+        fs.run_until(1.0)
