@@ -21,7 +21,7 @@
 #include "hipims_b200.h"
 #include "hipims_b200_fused.h"
 
-static_assert(sizeof(hb_adjoint_args) == 168, "hb_adjoint_args layout (ctypes mirror)");
+static_assert(sizeof(hb_adjoint_args) == 184, "hb_adjoint_args layout (ctypes mirror)");
 
 namespace hb {
 namespace {
@@ -156,6 +156,36 @@ __device__ FaceOut5 face_at(const Grid &G, const BcVals &bc, int ra, int ca, int
   return o;
 }
 
+// Face values kept by the optional face pass: x-face (r, c-1)|(r, c) and
+// y-face (r, c)|(r-1, c) of index r * (cols + 1) + c, fields fh, fx, fy, sa, sb.
+__device__ __forceinline__ FaceOut5 load_face(const hb_adjoint_args &a, int dir, int r, int c) {
+  const double *f = a.faces + (size_t)dir * 5 * a.face_stride + (size_t)r * (a.cols + 1) + c;
+  const int64_t s = a.face_stride;
+  return FaceOut5{f[0], f[s], f[2 * s], f[3 * s], f[4 * s]};
+}
+
+// Pass 0 (optional): every face once, forward only, into a.faces.
+__global__ void __launch_bounds__(128)
+adj_facefwd_kernel(hb_adjoint_args a) {
+  __shared__ BcVals bc;
+  const hb_instance &in = *a.instance;
+  Grid G{a.instance, a.rows, a.cols, a.pitch, a.code_pitch, a.h, a.qx, a.qy,
+         (const double *)in.z, in.code};
+  load_bc(in, a.t, bc);
+  __syncthreads();
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y * blockDim.y + threadIdx.y;
+  if (r > a.rows || c > a.cols) return;
+  const size_t idx = (size_t)r * (a.cols + 1) + c;
+  const int64_t s = a.face_stride;
+  FaceOut5 x{0, 0, 0, 0, 0}, y{0, 0, 0, 0, 0};
+  if (r < a.rows) x = face_at<0>(G, bc, r, c - 1, r, c, nullptr, nullptr, nullptr, nullptr);
+  if (c < a.cols) y = face_at<1>(G, bc, r, c, r - 1, c, nullptr, nullptr, nullptr, nullptr);
+  double *fx = a.faces + idx, *fy = a.faces + 5 * s + idx;
+  fx[0] = x.fh; fx[s] = x.fx; fx[2 * s] = x.fy; fx[3 * s] = x.sa; fx[4 * s] = x.sb;
+  fy[0] = y.fh; fy[s] = y.fx; fy[2 * s] = y.fy; fy[3 * s] = y.sa; fy[4 * s] = y.sb;
+}
+
 // Pass 1: per cell.
 __global__ void __launch_bounds__(256)
 adj_cell_kernel(hb_adjoint_args a) {
@@ -191,10 +221,18 @@ adj_cell_kernel(hb_adjoint_args a) {
       const double kk = a.dt / in.dx;
       C3 rr{0, 0, 0};
       if (active) {
-        const FaceOut5 fe = face_at<0>(G, bc, r, c, r, c + 1, nullptr, nullptr, nullptr, nullptr);
-        const FaceOut5 fw = face_at<0>(G, bc, r, c - 1, r, c, nullptr, nullptr, nullptr, nullptr);
-        const FaceOut5 fn = face_at<1>(G, bc, r, c, r - 1, c, nullptr, nullptr, nullptr, nullptr);
-        const FaceOut5 fs = face_at<1>(G, bc, r + 1, c, r, c, nullptr, nullptr, nullptr, nullptr);
+        FaceOut5 fe, fw, fn, fs;
+        if (a.faces) {
+          fe = load_face(a, 0, r, c + 1);
+          fw = load_face(a, 0, r, c);
+          fn = load_face(a, 1, r, c);
+          fs = load_face(a, 1, r + 1, c);
+        } else {
+          fe = face_at<0>(G, bc, r, c, r, c + 1, nullptr, nullptr, nullptr, nullptr);
+          fw = face_at<0>(G, bc, r, c - 1, r, c, nullptr, nullptr, nullptr, nullptr);
+          fn = face_at<1>(G, bc, r, c, r - 1, c, nullptr, nullptr, nullptr, nullptr);
+          fs = face_at<1>(G, bc, r + 1, c, r, c, nullptr, nullptr, nullptr, nullptr);
+        }
         rr.h = ((fw.fh + fs.fh) - (fe.fh + fn.fh)) * kk;
         rr.qx = ((fw.fx + fs.fx) - (fe.fx + fn.fx) - fe.sa + fw.sb) * kk;
         rr.qy = ((fw.fy + fs.fy) - (fe.fy + fn.fy) - fn.sa + fs.sb) * kk;
@@ -299,7 +337,16 @@ extern "C" int hb_adjoint_step(const hb_adjoint_args *a, void *stream) {
     return set_error(HB_ERR_ARG, "hb_adjoint_step: null pointer");
   if (a->rows <= 0 || a->cols <= 0 || a->pitch < a->cols + 8 || a->mu_stride <= 0)
     return set_error(HB_ERR_ARG, "hb_adjoint_step: bad geometry");
+  if (a->faces && a->face_stride < (int64_t)(a->rows + 1) * (a->cols + 1))
+    return set_error(HB_ERR_ARG, "hb_adjoint_step: face_stride below (rows + 1) * (cols + 1)");
   auto st = as_stream(stream);
+  if (a->faces) {
+    const dim3 blk0(32, 4);
+    const dim3 g0((a->cols + 1 + 31) / 32, (a->rows + 1 + 3) / 4);
+    adj_facefwd_kernel<<<g0, blk0, 0, st>>>(*a);
+    int rc0 = check_launch("hb_adjoint_step (faces forward)");
+    if (rc0) return rc0;
+  }
   const dim3 blk(32, 8);
   const dim3 g1((a->cols + 31) / 32, (a->rows + 7) / 8);
   adj_cell_kernel<<<g1, blk, 0, st>>>(*a);

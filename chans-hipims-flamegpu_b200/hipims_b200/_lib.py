@@ -92,6 +92,7 @@ class HbAdjointArgs(ctypes.Structure):
         ("mu", c_vp), ("mu_stride", c_i64), ("grad", c_vp),
         ("t", c_dbl), ("dt", c_dbl), ("rain_rate", c_dbl), ("rain_base", c_dbl),
         ("h_reg", c_dbl), ("first", c_i32), ("pad", c_i32),
+        ("faces", c_vp), ("face_stride", c_i64),
     ]
 
 

@@ -76,7 +76,8 @@ class GaugeMisfit:
 
     def __init__(self, catchment: Catchment, gauge_rows, gauge_cols, nsteps: int,
                  dt_schedule: np.ndarray, every: int = 10, checkpoint: int = 100,
-                 obs=None, weight: float = 1.0, h_reg: float = 1.0e-5, device="cuda"):
+                 obs=None, weight: float = 1.0, h_reg: float = 1.0e-5,
+                 store_faces: bool = True, device="cuda"):
         dts = np.asarray(dt_schedule, dtype=np.float64)
         if dts.shape[0] < nsteps:
             raise ValueError(f"dt schedule has {dts.shape[0]} steps, {nsteps} needed")
@@ -90,6 +91,7 @@ class GaugeMisfit:
         self.nsteps, self.every, self.K = int(nsteps), int(every), int(checkpoint)
         self.weight = float(weight)
         self.h_reg = float(h_reg)
+        self.store_faces = bool(store_faces)
         self.fs = FusedSolver(self.catchment, dtype=torch.float64, device=device)
         self.device = self.fs.device
         self.n_zones = len(catchment.manning)
@@ -180,6 +182,11 @@ class GaugeMisfit:
         a.rows, a.cols, a.pitch, a.code_pitch = ins.rows, ins.cols, ins.pitch, ins.code_pitch
         a.mu, a.mu_stride, a.grad = mu.data_ptr(), n, grad.data_ptr()
         a.h_reg = self.h_reg
+        faces = None
+        if self.store_faces:  # each face's forward values once per reverse step
+            stride = (ins.rows + 1) * (ins.cols + 1)
+            faces = torch.empty(10 * stride, dtype=torch.float64, device=dev)
+            a.faces, a.face_stride = faces.data_ptr(), stride
         ctrlf = self.fs.ctrl.view(torch.float64)
         with torch.cuda.device(dev):
             for s0 in sorted(self._ckpt, reverse=True):

@@ -188,6 +188,10 @@ typedef struct hb_adjoint_args {
                                          negative depths) */
   int32_t first;                      /* step n starts at t == 0 */
   int32_t pad;
+  double *faces;                      /* optional scratch, 10 * face_stride doubles: the
+                                         forward face values of step n, computed once
+                                         instead of twice per face; NULL: recomputed */
+  int64_t face_stride;                /* >= (rows + 1) * (cols + 1) */
 } hb_adjoint_args;
 int hb_adjoint_step(const hb_adjoint_args *args, void *stream);
 /* lam_h[offsets[i]] += 2 * weight * (h[offsets[i]] - obs[i]): the gradient of

@@ -59,7 +59,7 @@ def test_fused_rejects_bad_record():
 def test_adjoint_rejects_bad_arguments():
     L = _lib.lib()
     a = _lib.HbAdjointArgs()
-    assert ctypes.sizeof(a) == 168
+    assert ctypes.sizeof(a) == 184
     assert L.hb_adjoint_step(ctypes.byref(a), None) == -1
     assert b"null" in L.hb_last_error()
     assert L.hb_adjoint_gauge(-1, None, None, None, None, 1.0, None) == -1

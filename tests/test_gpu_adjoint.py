@@ -185,3 +185,20 @@ def test_dry_start_rain_case(cuda):
     assert stable.sum() >= (len(g) + 1) // 2, (f4, f5)
     err = np.abs(g - f5)[stable] / scale
     assert err.max() <= 1e-3, (g, f5, stable)
+
+
+def test_face_scratch_gives_the_same_gradient(case, cuda):
+    """The adjoint step with the face scratch (each face's forward values
+    computed once) and without it (recomputed inside the cell pass) agree."""
+    d, c, dts, p, start = case
+    q = GaugeMisfit(c, d["gauge_rows"], d["gauge_cols"], NSTEPS, dts, EVERY, K, obs=p.obs,
+                    store_faces=False, device=cuda)
+    q.simulate(start, 0.8)
+    p.simulate(start, 0.8)
+    gq, lq = q.gradient(with_state=True)
+    gp, lp = p.gradient(with_state=True)
+    # equal up to the summation order of the face pass's FP64 atomics
+    np.testing.assert_allclose(gp, gq, rtol=1e-10, atol=0)
+    for f in ("h", "qx", "qy"):
+        a, b = lp[f].cpu().numpy(), lq[f].cpu().numpy()
+        np.testing.assert_allclose(a, b, rtol=0, atol=1e-12 * np.abs(b).max())
