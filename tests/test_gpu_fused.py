@@ -377,3 +377,47 @@ def test_non_finite_state_is_reported(cuda):
         fs.check()
     with pytest.raises(FloatingPointError):
         fs.run_until(1.0)
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_fused_fp32_mixed_boundaries_high_bed(cuda, seed):
+    """FP32 on every ghost type with the bed 37.3 m up (a 37 m datum per block,
+    the WL_GIVEN table shifted with it), against the oracle with its dt
+    sequence replayed: the boundary values and the datum shift meet in the
+    ghost states."""
+    from hipims_b200.fused import FusedSolver
+
+    d = G.mixed_bc_case(300 + seed, 2)
+    d.pop("rain_mask")
+    d["rain"] = np.array([[0.0, 2e-4], [1.0, 5e-4], [10.0, 0.0]])
+    d["z"] = np.asarray(d["z"]) + 37.3
+    d["wl"] = np.asarray(d["wl"]) + 37.3
+    gw = np.array(d["given_wl"], dtype=np.float64)
+    gw[:, 1:] += 37.3
+    d["given_wl"] = gw
+    sim = O.Sim(d, order=2)
+    dts = sim.run_record(8)
+    fs = FusedSolver(catchment(d, dt_replay=dts), dtype=torch.float32, device=cuda)
+    assert float(fs.inst[0].datum_np.max()) == 37.0
+    fs.step(8)
+    err = compare(fs, sim)
+    print("mixed bc FP32 (bed +37.3 m) vs oracle after 8 steps:", err)
+    assert err["h"] < 1e-4 and err["qx"] < 1e-4 and err["qy"] < 1e-4, err
+
+
+def test_fused_fp32_channel_boundaries(cuda):
+    """H_GIVEN inflow, OPEN outflow, walls in FP32, the oracle's dt replayed
+    up to the case's end time (8 s, where the fused clock halts)."""
+    from hipims_b200 import scenarios as S
+    from hipims_b200.fused import FusedSolver
+
+    d = S.channel()
+    sim = O.Sim(d, order=2)
+    dts = sim.run_record(400, t_end=d["t_end"])
+    assert sim.g.t >= d["t_end"] and len(dts) > 200
+    fs = FusedSolver(catchment(d, dt_replay=dts), dtype=torch.float32, device=cuda)
+    fs.step(len(dts))
+    assert fs.controls()[0].halted == 1
+    err = compare(fs, sim)
+    print(f"channel FP32 vs oracle after {len(dts)} steps:", err)
+    assert err["h"] < 1e-4 and err["qx"] < 1e-4, err
