@@ -565,22 +565,38 @@ def coupled_rate(dev, n: int = 8192, sim_seconds: float = 120.0, period: float =
                     "chunk) + hb_gather of h, u, v + D2H + msgpack, wall clock"}
 
 
-def accuracy_vs_fp64(d: dict, dev, horizons=(64, 1000)) -> dict:
+def accuracy_vs_fp64(d: dict, dev, horizons=(64, 1000), times=(300.0, 600.0)) -> dict:
     """Max depth / velocity difference of the FP32 fused run against the FP64
     fused run at identical simulated times (the FP64 dt sequence replayed), and
-    the FP64 volume balance of the FP32 run, after each horizon (steps from
-    the dry start)."""
+    the FP64 volume balance of the FP32 run, after each horizon: the step
+    counts in `horizons` and the first steps that reach the simulated times in
+    `times` (from the dry start).
+
+    The horizons stop at 600 s of the 3600 s storm: from about 650 s on, the
+    reference scheme draws water in through the OPEN ring (its zero-gradient
+    ghost copies an edge cell whose velocity points inwards, so that cell never
+    drains), and isolated cells reach 50-300 m/s; the reference's own kernels,
+    the FP64 and the FP32 fused runs all do so, and their trajectories part
+    (different step counts to the same time), so no pointwise comparison is
+    meaningful there."""
     from hipims_b200.fused import FusedSolver
     from hipims_b200.scenarios import catchment_from
 
-    horizons = sorted(horizons)
     f64 = FusedSolver(catchment_from(d), dtype=torch.float64, device=dev)
-    dts, ref = [], {}
-    for k in range(1, horizons[-1] + 1):
+    dts, ref, k = [], {}, 0
+    steps_set, pending = set(horizons), sorted(times)
+    while k < max(horizons, default=0) or pending:
         f64.step(1)
-        dts.append(f64.controls()[0].dt)
-        if k in horizons:
+        k += 1
+        c = f64.controls()[0]
+        dts.append(c.dt)
+        hit = k in steps_set
+        while pending and c.t >= pending[0]:
+            pending.pop(0)
+            hit = True
+        if hit:
             ref[k] = f64.compacted()
+    horizons = sorted(ref)
     del f64
     # the scheme's own sensitivity: the FP64 run again with the bed scaled by
     # (1 + 1e-15), same dt sequence
@@ -613,6 +629,8 @@ def accuracy_vs_fp64(d: dict, dev, horizons=(64, 1000)) -> dict:
                     "cells_dh_over_1e-4": int((dh > 1e-4).sum()),
                     "cells_dh_over_1e-3": int((dh > 1e-3).sum()),
                     "max_abs_du_ms_wet": float(np.abs(ua - ub).max()),
+                    "flooded_cells_fp64": int((b["h"] > 0.1).sum()),
+                    "flooded_cells_differing": int(((a["h"] > 0.1) != (b["h"] > 0.1)).sum()),
                     "volume_balance_rel_err": bal,
                     "fp64_self_sensitivity_max_abs_dh_m": sens[k]})
     return {"horizons": out, "reference": "FP64 fused run, same dt sequence",
