@@ -42,6 +42,10 @@ namespace hb {
 namespace {
 
 constexpr int kNT = 256;  // threads per CTA
+// Tiles per reduction group of the rows kernel: the last tile of a group to
+// finish sums the group's partials (one per thread of a 128-thread CTA), and
+// the last group of an instance finalizes the step from the group sums.
+constexpr int kGroupTiles = 128;
 
 struct TilePartial {
   double smax;     // max CFL wave speed sqrt(g h) + max(|qx|, |qy|) / h over wet cells
@@ -200,17 +204,19 @@ __device__ __forceinline__ double warp_max(double v) {
 
 // Rain rate at t with the reference's monotone row cursor
 // (HP/SWE_CUDA.py:472-495): linear interpolation, zero after the last row.
-__device__ double rain_rate_at(const hb_instance &in, hb_ctrl *c, double t) {
+// The cursor and multiplier are read from `rd` (the control block or a
+// snapshot of it) and the moved cursor is written to `wr`.
+__device__ double rain_rate_at(const hb_instance &in, const hb_ctrl *rd, hb_ctrl *wr, double t) {
   if (!in.rain_tab || in.rain_rows < 2) return 0.0;
   const double *R = in.rain_tab;
   const int C = in.rain_cols;
   if (!(t < R[(int64_t)(in.rain_rows - 1) * C])) return 0.0;
-  int idx = min(max(c->rain_index, 0), in.rain_rows - 2);
+  int idx = min(max(rd->rain_index, 0), in.rain_rows - 2);
   while (idx + 2 < in.rain_rows && !(t < R[(int64_t)(idx + 1) * C])) idx++;
-  c->rain_index = idx;
+  wr->rain_index = idx;
   const double *r0 = R + (int64_t)idx * C, *r1 = r0 + C;
   const double per = (t - r0[0]) / (r1[0] - r0[0]);
-  return (r0[1] + per * (r1[1] - r0[1])) * c->rain_mult;
+  return (r0[1] + per * (r1[1] - r0[1])) * rd->rain_mult;
 }
 
 // Rates of every rain station at t (HP/SWE_CUDA.py:472-502: the row cursor
@@ -298,14 +304,17 @@ __device__ void bc_values_exact(const hb_instance &in, double t, BcTable *out) {
 // and the any-dry flag D (HC/timeControl_Kernel.cu:164-198 per cell, torch.min,
 // then HP/SWE_CUDA.py:818-831: 10x cap, export clip, t += dt), the rain rate
 // and the boundary values at the new t.  All threads of the block call it;
-// thread 0 owns the control block.
+// thread 0 owns the control block.  The step's clock fields are read from
+// `snap` (the control block itself, or a copy taken at the start of the
+// finalize) and the new values are written to the control block.
 template <typename T, int NT>
-__device__ void advance_clock(const hb_instance &in, int ii, BcTable *bct, double SM, int D) {
+__device__ void advance_clock(const hb_instance &in, int ii, BcTable *bct, double SM, int D,
+                              const hb_ctrl *snap) {
   const int tid = threadIdx.x;
   hb_ctrl *ctrl = in.ctrl;
   __shared__ double s_tnew;
   if (tid == 0) {
-    const double dtn = ctrl->dt, tn = ctrl->t;
+    const double dtn = snap->dt, tn = snap->t;
     // min over cells of CFL*dx/speed; the division is monotone, so dividing
     // once by the largest speed gives the same value.
     double cand = INFINITY;
@@ -314,20 +323,21 @@ __device__ void advance_clock(const hb_instance &in, int ii, BcTable *bct, doubl
     double dtnew = (cand == INFINITY) ? dtn : cand;
     const double upper = dtn * 10.0;
     if (upper < dtnew) dtnew = upper;  // Python min(self.dt, time_upper)
-    const double next_export = (double)(ctrl->export_n + 1) * ctrl->export_step;
-    if (ctrl->export_step > 0.0 && dtnew + tn >= next_export) {
+    const double next_export = (double)(snap->export_n + 1) * snap->export_step;
+    if (snap->export_step > 0.0 && dtnew + tn >= next_export) {
       dtnew = next_export - tn;
-      ctrl->export_n += 1;
-      ctrl->exports += 1;
-      if (ctrl->halt_on_export) ctrl->halted = 1;
+      ctrl->export_n = snap->export_n + 1;
+      ctrl->exports = snap->exports + 1;
+      if (snap->halt_on_export) ctrl->halted = 1;
     }
-    if (in.dt_replay && ctrl->step < in.n_replay) dtnew = in.dt_replay[ctrl->step];
-    if (!isfinite(dtnew)) ctrl->status |= 1;
+    const int64_t step = snap->step;
+    if (in.dt_replay && step < in.n_replay) dtnew = in.dt_replay[step];
+    if (!isfinite(dtnew)) atomicOr(&ctrl->status, 1);
     const double tnew = tn + dtnew;
     ctrl->dt = dtnew;
     ctrl->t = tnew;
-    ctrl->step += 1;
-    if (tnew >= ctrl->t_end) ctrl->halted = 1;
+    ctrl->step = step + 1;
+    if (tnew >= snap->t_end) ctrl->halted = 1;
     s_tnew = tnew;
   }
   __syncthreads();
@@ -359,7 +369,7 @@ __device__ void advance_clock(const hb_instance &in, int ii, BcTable *bct, doubl
     ctrl->bc_vals[k][2] = (float)qxb;
     ctrl->bc_vals[k][3] = (float)qyb;
   } else if (tid == 32) {
-    ctrl->rain_rate = rain_rate_at(in, ctrl, tnew);
+    ctrl->rain_rate = rain_rate_at(in, snap, ctrl, tnew);
   }
   if (in.rain_station) {
     __syncthreads();  // the rain cursor
@@ -371,23 +381,12 @@ __device__ void advance_clock(const hb_instance &in, int ii, BcTable *bct, doubl
 // outflow, largest wave speed, any dry cell), account the step's volumes,
 // flip the state buffer and advance the clock -- or, with external_dt,
 // leave the clock to hb_fused_finish and publish the speed and dry flag.
-template <typename T, int NT>
-__device__ void finalize_instance(const hb_instance &in, int ii, TilePartial *partials,
-                                  BcTable *bct, double (*red_d)[NT / 32], double *red_s,
-                                  int *red_i) {
+// Sum of partials within a block, in a fixed order (lanes by a butterfly,
+// then warps in index order): the result is in thread 0.
+template <int NT>
+__device__ TilePartial block_partial_sum(double v, double o, double sm, int dry,
+                                         double (*red_d)[NT / 32], double *red_s, int *red_i) {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  hb_ctrl *ctrl = in.ctrl;
-  __threadfence();
-  const int nt = in.tiles_x * in.tiles_y;
-  double v = 0, o = 0, sm = 0;
-  int dry = 0;
-  for (int k = tid; k < nt; k += NT) {
-    const TilePartial *pp = partials + in.tile_begin + k;
-    v += __ldcg(&pp->volume);
-    o += __ldcg(&pp->outflow);
-    sm = fmax(sm, __ldcg(&pp->smax));
-    dry |= __ldcg(&pp->any_dry);
-  }
   v = warp_sum(v);
   o = warp_sum(o);
   sm = warp_max(sm);
@@ -399,30 +398,68 @@ __device__ void finalize_instance(const hb_instance &in, int ii, TilePartial *pa
     red_i[wid] = dry;
   }
   __syncthreads();
+  TilePartial p;
+  p.volume = p.outflow = p.smax = 0.0;
+  p.any_dry = 0;
+  p.pad = 0;
+  if (tid == 0) {
+    for (int w = 0; w < NT / 32; w++) {
+      p.volume += red_d[0][w];
+      p.outflow += red_d[1][w];
+      p.smax = fmax(p.smax, red_s[w]);
+      p.any_dry |= red_i[w];
+    }
+  }
+  return p;
+}
+
+// The instance's step is complete: reduce its `np` partials (per tile, or
+// per group of tiles), account the step's volumes, flip the state buffer
+// and advance the clock -- or, with external_dt, leave the clock to
+// hb_fused_finish and publish the speed and dry flag.  The control block is
+// copied to shared memory first (one load per thread) so that the clock
+// logic does not wait on a chain of dependent global loads.
+template <typename T, int NT>
+__device__ void finalize_instance(const hb_instance &in, int ii, const TilePartial *parts,
+                                  int np, BcTable *bct, double (*red_d)[NT / 32], double *red_s,
+                                  int *red_i) {
+  static_assert(sizeof(hb_ctrl) % 8 == 0 && sizeof(hb_ctrl) / 8 <= NT, "control block copy");
+  const int tid = threadIdx.x;
+  hb_ctrl *ctrl = in.ctrl;
+  __shared__ hb_ctrl s_snap;
+  __threadfence();
+  if (tid < (int)(sizeof(hb_ctrl) / 8))
+    reinterpret_cast<unsigned long long *>(&s_snap)[tid] =
+        __ldcg(reinterpret_cast<const unsigned long long *>(ctrl) + tid);
+  double v = 0, o = 0, sm = 0;
+  int dry = 0;
+  for (int k = tid; k < np; k += NT) {
+    const TilePartial *pp = parts + k;
+    v += __ldcg(&pp->volume);
+    o += __ldcg(&pp->outflow);
+    sm = fmax(sm, __ldcg(&pp->smax));
+    dry |= __ldcg(&pp->any_dry);
+  }
+  const TilePartial P = block_partial_sum<NT>(v, o, sm, dry, red_d, red_s, red_i);
   __shared__ double s_sm;
   __shared__ int s_dry, s_ext;
   if (tid == 0) {
-    double V = 0, O = 0, SM = 0;
-    int D = 0;
-    for (int w = 0; w < NT / 32; w++) {
-      V += red_d[0][w];
-      O += red_d[1][w];
-      SM = fmax(SM, red_s[w]);
-      D |= red_i[w];
-    }
-    const double dtn = ctrl->dt, dxd = in.dx;
-    if (!isfinite(V)) ctrl->status |= 4;  // a NaN / inf depth somewhere in the raster
+    const hb_ctrl &c = s_snap;
+    const double V = P.volume, O = P.outflow, SM = P.smax;
+    const int D = P.any_dry;
+    const double dtn = c.dt, dxd = in.dx;
+    if (!isfinite(V)) atomicOr(&ctrl->status, 4);  // a NaN / inf depth somewhere in the raster
     ctrl->volume = V * dxd * dxd;
-    ctrl->outflow_volume += O * dtn * dxd;
+    ctrl->outflow_volume = c.outflow_volume + O * dtn * dxd;
     if (in.rain_station) {
       double rv = 0.0;
       for (int k = 0; k < in.n_stations; k++) rv += in.station_rate[k] * in.station_cells[k];
-      ctrl->rain_volume += rv * dtn * dxd * dxd;
+      ctrl->rain_volume = c.rain_volume + rv * dtn * dxd * dxd;
     } else {
-      ctrl->rain_volume += ctrl->rain_rate * dtn * dxd * dxd * (double)in.n_valid;
+      ctrl->rain_volume = c.rain_volume + c.rain_rate * dtn * dxd * dxd * (double)in.n_valid;
     }
-    ctrl->cur = 1 - ctrl->cur;
-    s_ext = ctrl->external_dt;
+    ctrl->cur = 1 - c.cur;
+    s_ext = c.external_dt;
     if (s_ext) {
       ctrl->ext[0] = SM;
       ctrl->ext[1] = D ? 1.0 : 0.0;
@@ -431,8 +468,39 @@ __device__ void finalize_instance(const hb_instance &in, int ii, TilePartial *pa
     s_dry = D;
   }
   __syncthreads();
-  if (!s_ext) advance_clock<T, NT>(in, ii, bct, s_sm, s_dry);
+  if (!s_ext) advance_clock<T, NT>(in, ii, bct, s_sm, s_dry, &s_snap);
   if (tid == 0) ctrl->tiles_done = 0u;
+}
+
+// The last tile of a group to finish: sum the group's `n` tile partials
+// (one per thread), store the group sum and count the group; the
+// instance's last group finalizes the step from the group sums.
+template <typename T, int NT>
+__device__ void close_group(const hb_instance &in, int ii, const TilePartial *tiles, int n,
+                            TilePartial *gparts, unsigned *gcount, int gi, int gbase, int ng,
+                            BcTable *bct, double (*red_d)[NT / 32], double *red_s, int *red_i,
+                            int *flag) {
+  static_assert(kGroupTiles <= NT, "one tile partial per thread");
+  const int tid = threadIdx.x;
+  __threadfence();
+  double v = 0, o = 0, sm = 0;
+  int dry = 0;
+  if (tid < n) {
+    const TilePartial *pp = tiles + tid;
+    v = __ldcg(&pp->volume);
+    o = __ldcg(&pp->outflow);
+    sm = __ldcg(&pp->smax);
+    dry = __ldcg(&pp->any_dry);
+  }
+  const TilePartial P = block_partial_sum<NT>(v, o, sm, dry, red_d, red_s, red_i);
+  if (tid == 0) {
+    gparts[gi] = P;
+    gcount[gi] = 0u;  // every tile of the group has counted: ready for the next step
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> done(in.ctrl->tiles_done);
+    *flag = (done.fetch_add(1u, cuda::memory_order_acq_rel) == (unsigned)(ng - 1));
+  }
+  __syncthreads();
+  if (*flag) finalize_instance<T, NT>(in, ii, gparts + gbase, ng, bct, red_d, red_s, red_i);
 }
 
 // hb_fused_finish: one block per instance advances the clock from the
@@ -444,17 +512,27 @@ finish_kernel(const hb_instance *__restrict__ insts, BcTable *__restrict__ bct,
   const hb_instance &in = insts[blockIdx.x];
   if (in.ctrl->halted) return;
   advance_clock<T, kNT>(in, blockIdx.x, bct, ext[2 * blockIdx.x],
-                        ext[2 * blockIdx.x + 1] != 0.0 ? 1 : 0);
+                        ext[2 * blockIdx.x + 1] != 0.0 ? 1 : 0, in.ctrl);
 }
 
-// Workspace layout: [n_tiles] TilePartial, [n_instances] BcTable, then
-// [n_instances][kMapsPerInstance] CUtensorMap (128-byte aligned).
-inline size_t ws_partials_bytes(int n_tiles) {
-  return ((size_t)n_tiles * sizeof(TilePartial) + 255) & ~(size_t)255;
+// Workspace layout (each part 256-byte aligned): [n_tiles] TilePartial,
+// [n_groups] TilePartial (sums of groups of kGroupTiles tiles), [n_groups]
+// unsigned group counters, [n_instances] BcTable, then
+// [n_instances][kMapsPerInstance] CUtensorMap.  Instance i's groups start at
+// tile_begin / kGroupTiles + i, which never overlaps instance i + 1's.
+inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+inline size_t ws_partials_bytes(int n_tiles) { return align256((size_t)n_tiles * sizeof(TilePartial)); }
+inline int ws_n_groups(const hb_fused_batch *b) {
+  return b->n_tiles / kGroupTiles + b->n_instances + 1;
+}
+inline size_t ws_gcount_offset(const hb_fused_batch *b) {
+  return ws_partials_bytes(b->n_tiles) + align256((size_t)ws_n_groups(b) * sizeof(TilePartial));
+}
+inline size_t ws_bct_offset(const hb_fused_batch *b) {
+  return ws_gcount_offset(b) + align256((size_t)ws_n_groups(b) * sizeof(unsigned));
 }
 inline size_t ws_maps_offset(const hb_fused_batch *b) {
-  return (ws_partials_bytes(b->n_tiles) + (size_t)b->n_instances * sizeof(BcTable) + 255) &
-         ~(size_t)255;
+  return align256(ws_bct_offset(b) + (size_t)b->n_instances * sizeof(BcTable));
 }
 
 // ---------------------------------------------------------------------------
@@ -780,7 +858,9 @@ fused_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restri
     }
     __syncthreads();
 
-    if (s.last) finalize_instance<T, kNT>(in, ii, partials, bct, s.red_d, s.red_s, s.red_i);
+    if (s.last)
+      finalize_instance<T, kNT>(in, ii, partials + in.tile_begin, in.tiles_x * in.tiles_y, bct,
+                                s.red_d, s.red_s, s.red_i);
     __syncthreads();
   }
 }
@@ -829,6 +909,7 @@ struct RowsSmem {
   double red_s[kRowsNW];
   int red_i[kRowsNW];
   int last;
+  int last2;
   static constexpr unsigned kTxBytes =
       (unsigned)(4 * SH * kSWF * sizeof(T) + TY * kTW * sizeof(T) + SH * kSWC);
 };
@@ -1051,7 +1132,8 @@ __device__ __forceinline__ FaceOut<T> face_any(const RowsSmem<T, TY> &s, const C
 template <typename T, int TY, bool FAST, int MINB, bool SOURCES = false>
 __global__ void __launch_bounds__(kRowsNT, MINB)
 rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restrict__ tile_inst,
-                 int n_tiles, TilePartial *__restrict__ partials, BcTable *__restrict__ bct,
+                 int n_tiles, TilePartial *__restrict__ partials, TilePartial *__restrict__ gparts,
+                 unsigned *__restrict__ gcount, BcTable *__restrict__ bct,
                  const CUtensorMap *__restrict__ maps) {
   using S = RowsSmem<T, TY>;
   constexpr int R = S::R;
@@ -1415,6 +1497,10 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
       s.red_i[w] = any_dry;
     }
     __syncthreads();
+    const int n_inst_tiles = in.tiles_x * in.tiles_y;
+    const int grp = lt / kGroupTiles;
+    const int gsize = min(kGroupTiles, n_inst_tiles - grp * kGroupTiles);
+    const int gbase = in.tile_begin / kGroupTiles + ii;
     if (tid == 0) {
       TilePartial p;
       p.volume = p.outflow = p.smax = 0.0;
@@ -1427,13 +1513,16 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
         p.any_dry |= s.red_i[q];
       }
       partials[tile] = p;
-      const unsigned n_inst_tiles = (unsigned)(in.tiles_x * in.tiles_y);
-      // release: this tile's partial is visible before the count moves
-      cuda::atomic_ref<unsigned, cuda::thread_scope_device> done(ctrl->tiles_done);
-      s.last = (done.fetch_add(1u, cuda::memory_order_acq_rel) == n_inst_tiles - 1);
+      // release: this tile's partial is visible before its group's count moves
+      cuda::atomic_ref<unsigned, cuda::thread_scope_device> done(gcount[gbase + grp]);
+      s.last = (done.fetch_add(1u, cuda::memory_order_acq_rel) == (unsigned)(gsize - 1));
     }
     __syncthreads();
-    if (s.last) finalize_instance<T, kRowsNT>(in, ii, partials, bct, s.red_d, s.red_s, s.red_i);
+    if (s.last)
+      close_group<T, kRowsNT>(in, ii, partials + in.tile_begin + grp * kGroupTiles, gsize,
+                              gparts, gcount, gbase + grp, gbase,
+                              (n_inst_tiles + kGroupTiles - 1) / kGroupTiles, bct, s.red_d,
+                              s.red_s, s.red_i, &s.last2);
     __syncthreads();
   }
 }
@@ -1449,7 +1538,7 @@ prepare_kernel(const hb_instance *__restrict__ insts, BcTable *__restrict__ bct)
     c->volume = 0.0;
     c->volume0 = 0.0;
     c->tiles_done = 0u;
-    c->rain_rate = rain_rate_at(in, c, c->t);
+    c->rain_rate = rain_rate_at(in, c, c, c->t);
     bc_values_exact(in, c->t, &bct[blockIdx.x]);
     bc_values_at(in, c, c->t);
   }
@@ -1513,7 +1602,7 @@ int launch_steps(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   int grid = b->grid_blocks > 0 ? b->grid_blocks : blocks_per_sm * num_sms();
   if (grid > b->n_tiles) grid = b->n_tiles;
   TilePartial *parts = reinterpret_cast<TilePartial *>(b->workspace);
-  BcTable *bct = reinterpret_cast<BcTable *>((char *)b->workspace + ws_partials_bytes(b->n_tiles));
+  BcTable *bct = reinterpret_cast<BcTable *>((char *)b->workspace + ws_bct_offset(b));
   for (int k = 0; k < nsteps; k++) {
     fused_step_kernel<T, TY, TX, FAST><<<grid, kNT, sizeof(S), st>>>(
         b->instances, b->tile_instance, b->n_tiles, parts, bct);
@@ -1537,15 +1626,22 @@ int launch_rows_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   });
   if (attr_err != cudaSuccess)
     return set_error(HB_ERR_CUDA, "fused step setup: %s", cudaGetErrorString(attr_err));
-  int grid = b->grid_blocks > 0 ? b->grid_blocks : blocks_per_sm * num_sms();
+  // one CTA per tile by default: the block scheduler starts the next tile as
+  // soon as a CTA retires, which balances tiles of uneven cost (boundary
+  // columns, wet fronts) better than a fixed share per resident CTA; a
+  // positive grid_blocks makes the CTAs loop over tiles instead
+  (void)blocks_per_sm;
+  int grid = b->grid_blocks > 0 ? b->grid_blocks : b->n_tiles;
   if (grid > b->n_tiles) grid = b->n_tiles;
   char *ws = reinterpret_cast<char *>(b->workspace);
   TilePartial *parts = reinterpret_cast<TilePartial *>(ws);
-  BcTable *bct = reinterpret_cast<BcTable *>(ws + ws_partials_bytes(b->n_tiles));
+  TilePartial *gparts = reinterpret_cast<TilePartial *>(ws + ws_partials_bytes(b->n_tiles));
+  unsigned *gcount = reinterpret_cast<unsigned *>(ws + ws_gcount_offset(b));
+  BcTable *bct = reinterpret_cast<BcTable *>(ws + ws_bct_offset(b));
   const CUtensorMap *maps = reinterpret_cast<const CUtensorMap *>(ws + ws_maps_offset(b));
   for (int k = 0; k < nsteps; k++) {
     rows_step_kernel<T, TY, FAST, MINB, SOURCES><<<grid, kRowsNT, sizeof(S), st>>>(
-        b->instances, b->tile_instance, b->n_tiles, parts, bct, maps);
+        b->instances, b->tile_instance, b->n_tiles, parts, gparts, gcount, bct, maps);
   }
   return check_launch("hb_fused_step");
 }
@@ -1677,7 +1773,15 @@ int prepare_impl(const hb_fused_batch *b, cudaStream_t st, CUtensorMap *host_map
                                      "station rain; set HB_FLAG_SOURCES", i);
     }
   }
-  BcTable *bct = reinterpret_cast<BcTable *>((char *)b->workspace + ws_partials_bytes(b->n_tiles));
+  BcTable *bct = reinterpret_cast<BcTable *>((char *)b->workspace + ws_bct_offset(b));
+  // the rows kernel's group counters start at zero; each group's last tile
+  // resets its counter for the next step
+  if (b->n_tiles > 0) {
+    const cudaError_t e = cudaMemsetAsync((char *)b->workspace + ws_gcount_offset(b), 0,
+                                          (size_t)ws_n_groups(b) * sizeof(unsigned), st);
+    if (e != cudaSuccess)
+      return set_error(HB_ERR_CUDA, "hb_fused_prepare: %s", cudaGetErrorString(e));
+  }
   // blocks per instance for the volume sum: about 16 cells per thread of the
   // largest instance (the host copy of the records gives the sizes)
   int64_t most = (int64_t)1 << 22;
@@ -1710,7 +1814,7 @@ extern "C" int hb_fused_prepare(const hb_fused_batch *b, void *stream) {
 extern "C" int hb_fused_finish(const hb_fused_batch *b, const double *ext, void *stream) {
   if (!b || !b->instances || !b->workspace || b->n_instances <= 0 || !ext)
     return set_error(HB_ERR_ARG, "hb_fused_finish: bad batch record or null ext");
-  BcTable *bct = reinterpret_cast<BcTable *>((char *)b->workspace + ws_partials_bytes(b->n_tiles));
+  BcTable *bct = reinterpret_cast<BcTable *>((char *)b->workspace + ws_bct_offset(b));
   auto st = as_stream(stream);
   if (b->dtype == HB_F64)
     finish_kernel<double><<<b->n_instances, kNT, 0, st>>>(b->instances, bct, ext);

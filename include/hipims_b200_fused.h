@@ -136,7 +136,9 @@ typedef struct hb_fused_batch {
   int32_t n_instances;
   int32_t n_tiles;           /* sum of tiles_x * tiles_y */
   int32_t tile_y, tile_x;    /* tile shape: 32 wide, 32 or 64 high */
-  int32_t grid_blocks;       /* 0: one wave of resident blocks */
+  int32_t grid_blocks;       /* 0: one block per tile (rows kernel), one wave of resident
+                                blocks (tile-task kernel); > 0: that many blocks, each
+                                looping over tiles */
   int32_t order;             /* 2 (MUSCL); 1 (bed-only minmod) */
   int32_t flags;             /* HB_FLAG_* bits */
   const hb_instance *instances;  /* device [n_instances] */
