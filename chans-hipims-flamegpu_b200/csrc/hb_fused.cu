@@ -98,6 +98,11 @@ __device__ __forceinline__ Cell<T> sm_cell(const Smem<T, TY, TX> &s, int k) {
 
 __device__ __forceinline__ bool is_valid(uint8_t code) { return (code >> 4) != HB_NODATA_CLASS; }
 
+template <bool B>
+struct BoolTag {
+  static constexpr bool value = B;
+};
+
 // Interior face between valid cells A (west/south) and B (east/north),
 // evaluated from A's side with normal +x (DIR 0) or +y (DIR 1, towards the
 // row above).  kl / krr: opposite neighbours of A / B (may be no-data).
@@ -1108,10 +1113,12 @@ struct RowsView {
 
 // Face between A (minus side) and B (plus side) along DIR, any validity.
 // sA / sB: MUSCL slopes of A and B along DIR (used only when both are valid).
-template <typename T, bool FAST, int DIR, int TY>
+// ALLV: both cells are known to be valid (no ghost face can occur).
+template <typename T, bool FAST, int DIR, int TY, bool ALLV = false>
 __device__ __forceinline__ FaceOut<T> face_any(const RowsSmem<T, TY> &s, const Cell<T> &A,
                                                uint8_t ca, const Cell<T> &B, uint8_t cb,
                                                const Slope<T> &sA, const Slope<T> &sB, T datum) {
+  if constexpr (ALLV) return face_edges<T, FAST, DIR>(A, B, sA, sB);
   const bool va = is_valid(ca), vb = is_valid(cb);
   if (va && vb) return face_edges<T, FAST, DIR>(A, B, sA, sB);
   FaceOut<T> o{T(0), T(0), T(0), T(0), T(0)};
@@ -1228,7 +1235,22 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
         if (dyb != 1 || dxb != 1) s.f[3][V.fi(i, j)] += s.ddatum[dyb * 3 + dxb];
       }
     }
-    __syncthreads();
+    // All-valid tile: every staged code of rows -2..TY+1, columns -4..35 is a
+    // valid cell and the cell-0 rule's cell is out of reach.  The row loop
+    // then runs with each validity test a compile-time true: the same
+    // arithmetic without no-data selects, ghost-face branches or
+    // boundary-outflow terms.
+    bool ok = !(bug_y >= y0 - 2 && bug_y <= y0 + TY + 1 && bug_x >= x0 - 4 && bug_x <= x0 + 35);
+    {
+      constexpr unsigned kNoData4 = 0x01010101u * (unsigned)(HB_NODATA_CLASS << 4);
+      const unsigned *cw = reinterpret_cast<const unsigned *>(s.code);
+      // 10 words per staged code row: bytes 12..51 are columns -4..35
+      for (int k = tid; k < S::SH * 10; k += kRowsNT) {
+        const unsigned w4 = cw[(k / 10) * (kSWC / 4) + 3 + k % 10];
+        ok = ok && (__vcmpeq4(w4 & 0xF0F0F0F0u, kNoData4) == 0u);
+      }
+    }
+    const bool allv = __syncthreads_and(ok) != 0;
 
     const int r0 = w * R;
     // --- tile edges, all lanes busy: warp 0 evaluates the faces between
@@ -1258,232 +1280,252 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
       }
     }
 
-    // --- column window: rows r0-2 .. r0+2
-    const int j = lane;
-    Cell<T> cN = V.cell(r0 - 1, j), cC = V.cell(r0, j), cS = V.cell(r0 + 1, j);
-    uint8_t kN = V.code(r0 - 1, j), kC = V.code(r0, j), kS = V.code(r0 + 1, j);
-    Slope<T> syC, syS;
-    FaceOut<T> nf;
-    {
-      const Cell<T> cNN = V.cell(r0 - 2, j);
-      const uint8_t kNN = V.code(r0 - 2, j);
-      const Cell<T> cSS = V.cell(r0 + 2, j);
-      const uint8_t kSS = V.code(r0 + 2, j);
-      // y-slopes: minus side = south (row + 1), plus side = north (row - 1)
-      const Slope<T> syN = slope_of(cN, cC, is_valid(kC), cNN, is_valid(kNN));
-      syC = slope_of(cC, cS, is_valid(kS), cN, is_valid(kN));
-      syS = slope_of(cS, cSS, is_valid(kSS), cC, is_valid(kC));
-      // face between rows r0-1 (north) and r0 (south), from the south side
-      nf = face_any<T, FAST, 1>(s, cC, kC, cN, kN, syC, syN, datum_tile);
-    }
-    __syncthreads();  // tile-edge faces and slopes ready
     // per-thread partial sums over this warp's rows (<= 16 cells) in T; the
     // tile and instance reductions are FP64
     T vol_t = T(0), smax_t = T(0);
     double outf = 0.0;
     int any_dry = 0;
-    T *hout = (T *)in.h[1 - cur];
-    T *qxout = (T *)in.qx[1 - cur];
-    T *qyout = (T *)in.qy[1 - cur];
-    T *hmaxg = (T *)in.h_max;
-    const int rx = x0 + j;
-    // read once per tile: the state stores below may alias the record
-    // (instances without infiltration or station rain take the SOURCES = false
-    // build, in which both branches vanish)
-    const bool infil = SOURCES && in.cum != nullptr;
-    const bool stations = SOURCES && in.rain_station != nullptr;
+    auto rows = [&](auto allv_tag) {
+      constexpr bool ALLV = decltype(allv_tag)::value;
+      auto valid = [](uint8_t k) -> bool {
+        if constexpr (ALLV) {
+          (void)k;
+          return true;
+        } else {
+          return is_valid(k);
+        }
+      };
+      // --- column window: rows r0-2 .. r0+2
+      const int j = lane;
+      Cell<T> cN = V.cell(r0 - 1, j), cC = V.cell(r0, j), cS = V.cell(r0 + 1, j);
+      uint8_t kN = V.code(r0 - 1, j), kC = V.code(r0, j), kS = V.code(r0 + 1, j);
+      Slope<T> syC, syS;
+      FaceOut<T> nf;
+      {
+        const Cell<T> cNN = V.cell(r0 - 2, j);
+        const uint8_t kNN = V.code(r0 - 2, j);
+        const Cell<T> cSS = V.cell(r0 + 2, j);
+        const uint8_t kSS = V.code(r0 + 2, j);
+        // y-slopes: minus side = south (row + 1), plus side = north (row - 1)
+        const Slope<T> syN = slope_of(cN, cC, valid(kC), cNN, valid(kNN));
+        syC = slope_of(cC, cS, valid(kS), cN, valid(kN));
+        syS = slope_of(cS, cSS, valid(kSS), cC, valid(kC));
+        // face between rows r0-1 (north) and r0 (south), from the south side
+        nf = face_any<T, FAST, 1, TY, ALLV>(s, cC, kC, cN, kN, syC, syN, datum_tile);
+      }
+      __syncthreads();  // tile-edge faces and slopes ready
+      T *hout = (T *)in.h[1 - cur];
+      T *qxout = (T *)in.qx[1 - cur];
+      T *qyout = (T *)in.qy[1 - cur];
+      T *hmaxg = (T *)in.h_max;
+      const int rx = x0 + j;
+      // read once per tile: the state stores below may alias the record
+      // (instances without infiltration or station rain take the SOURCES = false
+      // build, in which both branches vanish)
+      const bool infil = SOURCES && in.cum != nullptr;
+      const bool stations = SOURCES && in.rain_station != nullptr;
 
-#pragma unroll 1
-    for (int i = r0; i < r0 + R; ++i) {
-      const Cell<T> cW = V.cell(i, j - 1), cE = V.cell(i, j + 1);
-      const uint8_t kW = V.code(i, j - 1), kE = V.code(i, j + 1);
-      const bool vW = is_valid(kW), vE = is_valid(kE), vC = is_valid(kC);
-      const Slope<T> sxC = slope_of(cC, cW, vW, cE, vE);
-      Slope<T> sxW;
-      sxW.h = __shfl_up_sync(0xffffffffu, sxC.h, 1);
-      sxW.z = __shfl_up_sync(0xffffffffu, sxC.z, 1);
-      sxW.qx = __shfl_up_sync(0xffffffffu, sxC.qx, 1);
-      sxW.qy = __shfl_up_sync(0xffffffffu, sxC.qy, 1);
-      if (lane == 0) {
-        sxW.h = s.sxw[i][0];
-        sxW.z = s.sxw[i][1];
-        sxW.qx = s.sxw[i][2];
-        sxW.qy = s.sxw[i][3];
-      }
-      // west face (this cell is B) -> the west neighbour's east face
-      const FaceOut<T> wf = face_any<T, FAST, 0>(s, cW, kW, cC, kC, sxW, sxC, datum_tile);
-      T ef_h = __shfl_down_sync(0xffffffffu, wf.fh, 1);
-      T ef_x = __shfl_down_sync(0xffffffffu, wf.fx, 1);
-      T ef_y = __shfl_down_sync(0xffffffffu, wf.fy, 1);
-      T ef_a = __shfl_down_sync(0xffffffffu, wf.sa, 1);
-      if (lane == 31) {
-        ef_h = s.xe[i][0];
-        ef_x = s.xe[i][1];
-        ef_y = s.xe[i][2];
-        ef_a = s.xe[i][3];
-      }
-      // south face (this cell is B, the row below is A)
-      const FaceOut<T> sf = face_any<T, FAST, 1>(s, cS, kS, cC, kC, syS, syC, datum_tile);
-      const int ry = y0 + i;
-      if (vC) {
-        const T hc = cC.h;
-        bool active = first || hc > hs;
-        if (!active) {
-          const bool bugE = (ry == bug_y && rx + 1 == bug_x);
-          const bool bugW = (ry == bug_y && rx - 1 == bug_x);
-          const bool bugN = (ry - 1 == bug_y && rx == bug_x);
-          const bool bugS = (ry + 1 == bug_y && rx == bug_x);
-          active = (vE && !bugE && cE.h > hs) || (is_valid(kN) && !bugN && cN.h > hs) ||
-                   (vW && !bugW && cW.h > hs) || (is_valid(kS) && !bugS && cS.h > hs);
+  #pragma unroll 1
+      for (int i = r0; i < r0 + R; ++i) {
+        const Cell<T> cW = V.cell(i, j - 1), cE = V.cell(i, j + 1);
+        const uint8_t kW = V.code(i, j - 1), kE = V.code(i, j + 1);
+        const bool vW = valid(kW), vE = valid(kE), vC = valid(kC);
+        const Slope<T> sxC = slope_of(cC, cW, vW, cE, vE);
+        Slope<T> sxW;
+        sxW.h = __shfl_up_sync(0xffffffffu, sxC.h, 1);
+        sxW.z = __shfl_up_sync(0xffffffffu, sxC.z, 1);
+        sxW.qx = __shfl_up_sync(0xffffffffu, sxC.qx, 1);
+        sxW.qy = __shfl_up_sync(0xffffffffu, sxC.qy, 1);
+        if (lane == 0) {
+          sxW.h = s.sxw[i][0];
+          sxW.z = s.sxw[i][1];
+          sxW.qx = s.sxw[i][2];
+          sxW.qy = s.sxw[i][3];
         }
-        T hu = T(0), qxu = T(0), qyu = T(0);
-        if (active) {
-          if constexpr (FAST) {
-            const T r = dt / dx;
-            hu = ((wf.fh + sf.fh) - (ef_h + nf.fh)) * r;
-            qxu = ((wf.fx + sf.fx) - (ef_x + nf.fx) - ef_a + wf.sb) * r;
-            qyu = ((wf.fy + sf.fy) - (ef_y + nf.fy) - nf.sa + sf.sb) * r;
+        // west face (this cell is B) -> the west neighbour's east face
+        const FaceOut<T> wf = face_any<T, FAST, 0, TY, ALLV>(s, cW, kW, cC, kC, sxW, sxC, datum_tile);
+        T ef_h = __shfl_down_sync(0xffffffffu, wf.fh, 1);
+        T ef_x = __shfl_down_sync(0xffffffffu, wf.fx, 1);
+        T ef_y = __shfl_down_sync(0xffffffffu, wf.fy, 1);
+        T ef_a = __shfl_down_sync(0xffffffffu, wf.sa, 1);
+        if (lane == 31) {
+          ef_h = s.xe[i][0];
+          ef_x = s.xe[i][1];
+          ef_y = s.xe[i][2];
+          ef_a = s.xe[i][3];
+        }
+        // south face (this cell is B, the row below is A)
+        const FaceOut<T> sf = face_any<T, FAST, 1, TY, ALLV>(s, cS, kS, cC, kC, syS, syC, datum_tile);
+        const int ry = y0 + i;
+        if (vC) {
+          const T hc = cC.h;
+          bool active = first || hc > hs;
+          if (!active) {
+            if constexpr (ALLV) {
+              active = cE.h > hs || cN.h > hs || cW.h > hs || cS.h > hs;
+            } else {
+              const bool bugE = (ry == bug_y && rx + 1 == bug_x);
+              const bool bugW = (ry == bug_y && rx - 1 == bug_x);
+              const bool bugN = (ry - 1 == bug_y && rx == bug_x);
+              const bool bugS = (ry + 1 == bug_y && rx == bug_x);
+              active = (vE && !bugE && cE.h > hs) || (valid(kN) && !bugN && cN.h > hs) ||
+                       (vW && !bugW && cW.h > hs) || (valid(kS) && !bugS && cS.h > hs);
+            }
+          }
+          T hu = T(0), qxu = T(0), qyu = T(0);
+          if (active) {
+            if constexpr (FAST) {
+              const T r = dt / dx;
+              hu = ((wf.fh + sf.fh) - (ef_h + nf.fh)) * r;
+              qxu = ((wf.fx + sf.fx) - (ef_x + nf.fx) - ef_a + wf.sb) * r;
+              qyu = ((wf.fy + sf.fy) - (ef_y + nf.fy) - nf.sa + sf.sb) * r;
+            } else {
+              hu -= (ef_h / dx) * dt;
+              qxu -= (ef_x / dx) * dt;
+              qyu -= (ef_y / dx) * dt;
+              qxu -= (ef_a / dx) * dt;
+              hu -= (nf.fh / dx) * dt;
+              qxu -= (nf.fx / dx) * dt;
+              qyu -= (nf.fy / dx) * dt;
+              qyu -= (nf.sa / dx) * dt;
+              hu -= (-wf.fh / dx) * dt;
+              qxu -= (-wf.fx / dx) * dt;
+              qyu -= (-wf.fy / dx) * dt;
+              qxu -= (-wf.sb / dx) * dt;
+              hu -= (-sf.fh / dx) * dt;
+              qxu -= (-sf.fx / dx) * dt;
+              qyu -= (-sf.fy / dx) * dt;
+              qyu -= (-sf.sb / dx) * dt;
+            }
+            const bool bE = !vE, bW = !vW, bN = !valid(kN), bS = !valid(kS);
+            if (bE | bW | bN | bS) {
+              double o = 0.0;
+              if (bE) o += (double)ef_h;
+              if (bN) o += (double)nf.fh;
+              if (bW) o -= (double)wf.fh;
+              if (bS) o -= (double)sf.fh;
+              outf += o;
+            }
+          }
+          if (stations) {
+            // station rain (HC/stationPrecipitation_Kernel.cu:18-29), every valid cell
+            const size_t gs = (size_t)(ry + HB_PAD_Y) * P + (rx + HB_PAD_X);
+            hu += (T)in.station_rate[in.rain_station[gs]] * dt;
           } else {
-            hu -= (ef_h / dx) * dt;
-            qxu -= (ef_x / dx) * dt;
-            qyu -= (ef_y / dx) * dt;
-            qxu -= (ef_a / dx) * dt;
-            hu -= (nf.fh / dx) * dt;
-            qxu -= (nf.fx / dx) * dt;
-            qyu -= (nf.fy / dx) * dt;
-            qyu -= (nf.sa / dx) * dt;
-            hu -= (-wf.fh / dx) * dt;
-            qxu -= (-wf.fx / dx) * dt;
-            qyu -= (-wf.fy / dx) * dt;
-            qxu -= (-wf.sb / dx) * dt;
-            hu -= (-sf.fh / dx) * dt;
-            qxu -= (-sf.fx / dx) * dt;
-            qyu -= (-sf.fy / dx) * dt;
-            qyu -= (-sf.sb / dx) * dt;
+            hu += rain * dt;
           }
-          const bool bE = !vE, bW = !vW, bN = !is_valid(kN), bS = !is_valid(kS);
-          if (bE | bW | bN | bS) {
-            double o = 0.0;
-            if (bE) o += (double)ef_h;
-            if (bN) o += (double)nf.fh;
-            if (bW) o -= (double)wf.fh;
-            if (bS) o -= (double)sf.fh;
-            outf += o;
+          if (infil && active) {
+            // Green-Ampt infiltration on the flux list, after rain
+            // (HC/infiltrationCUDA_Kernel.cu:20-46; order HP/CatchFlood_main.py:164-170)
+            T *cum = (T *)in.cum + (size_t)(ry + HB_PAD_Y) * P + (rx + HB_PAD_X);
+            const int zc = kC & 15;
+            const T K = (T)in.ks[zc], psi = (T)in.psi[zc], dth = (T)in.dtheta[zc];
+            const T F0 = *cum;
+            const T a = F0 + dt * K;
+            const T F1 = T(0.5) * (a + sqrt(a * a + T(4) * dt * K * (psi + hc) * dth));
+            const T dF = fmin(hc, F1 - F0);
+            *cum = F0 + dF;
+            hu -= dF;
           }
-        }
-        if (stations) {
-          // station rain (HC/stationPrecipitation_Kernel.cu:18-29), every valid cell
-          const size_t gs = (size_t)(ry + HB_PAD_Y) * P + (rx + HB_PAD_X);
-          hu += (T)in.station_rate[in.rain_station[gs]] * dt;
-        } else {
-          hu += rain * dt;
-        }
-        if (infil && active) {
-          // Green-Ampt infiltration on the flux list, after rain
-          // (HC/infiltrationCUDA_Kernel.cu:20-46; order HP/CatchFlood_main.py:164-170)
-          T *cum = (T *)in.cum + (size_t)(ry + HB_PAD_Y) * P + (rx + HB_PAD_X);
-          const int zc = kC & 15;
-          const T K = (T)in.ks[zc], psi = (T)in.psi[zc], dth = (T)in.dtheta[zc];
-          const T F0 = *cum;
-          const T a = F0 + dt * K;
-          const T F1 = T(0.5) * (a + sqrt(a * a + T(4) * dt * K * (psi + hc) * dth));
-          const T dF = fmin(hc, F1 - F0);
-          *cum = F0 + dF;
-          hu -= dF;
-        }
-        T h = hc + hu;
-        T qx = cC.qx, qy = cC.qy;
-        T sgh = T(0);
-        T ih = T(0);
-        if (h < hs) {
-          qx = T(0);
-          qy = T(0);
-        } else {
-          const T n = s.manning[kC & 15];
-          qx += qxu;
-          qy += qyu;
-          sgh = FAST ? (T)sqrtf((float)(g * h)) : (T)__fsqrt_rn((float)(g * h));
-          if constexpr (FAST) {
-            ih = T(1) / h;
-            if (n > T(0)) {
-              const T q_norm = sqrtf(qx * qx + qy * qy);
-              const T a = dt * g * n * n * exp2f(-__log2f(h) * (T(1) / T(3))) * ih * ih;
-              const T fct = T(2) / (T(1) + sqrtf(T(1) + T(4) * a * q_norm));
-              const T lim = T(5) * h * sgh;
-              if (fabsf(qx) > T(1.0e-10)) {
-                const T temp = qx * fct;
-                if (fabsf(temp) > lim) {
-                  qx = T(2) * temp - qx;
-                  if (qx * temp <= T(0)) qx = T(0);
-                } else {
-                  qx = temp;
+          T h = hc + hu;
+          T qx = cC.qx, qy = cC.qy;
+          T sgh = T(0);
+          T ih = T(0);
+          if (h < hs) {
+            qx = T(0);
+            qy = T(0);
+          } else {
+            const T n = s.manning[kC & 15];
+            qx += qxu;
+            qy += qyu;
+            sgh = FAST ? (T)sqrtf((float)(g * h)) : (T)__fsqrt_rn((float)(g * h));
+            if constexpr (FAST) {
+              ih = T(1) / h;
+              if (n > T(0)) {
+                const T q_norm = sqrtf(qx * qx + qy * qy);
+                const T a = dt * g * n * n * exp2f(-__log2f(h) * (T(1) / T(3))) * ih * ih;
+                const T fct = T(2) / (T(1) + sqrtf(T(1) + T(4) * a * q_norm));
+                const T lim = T(5) * h * sgh;
+                if (fabsf(qx) > T(1.0e-10)) {
+                  const T temp = qx * fct;
+                  if (fabsf(temp) > lim) {
+                    qx = T(2) * temp - qx;
+                    if (qx * temp <= T(0)) qx = T(0);
+                  } else {
+                    qx = temp;
+                  }
+                }
+                if (fabsf(qy) > T(1.0e-10)) {
+                  const T temp = qy * fct;
+                  if (fabsf(temp) > lim) {
+                    qy = T(2) * temp - qy;
+                    if (qy * temp <= T(0)) qy = T(0);
+                  } else {
+                    qy = temp;
+                  }
                 }
               }
-              if (fabsf(qy) > T(1.0e-10)) {
-                const T temp = qy * fct;
-                if (fabsf(temp) > lim) {
-                  qy = T(2) * temp - qy;
-                  if (qy * temp <= T(0)) qy = T(0);
-                } else {
-                  qy = temp;
+            } else {
+              const T C_f = g * n * n * pow(h, T(-1.0 / 3.0));
+              const T q_norm = sqrt(qx * qx + qy * qy);
+              if (n > T(0)) {
+                if (fabs(qx) > T(1.0e-10)) {
+                  T temp = (T(1) - sqrt(T(1) + (T(4) * dt * C_f) / (h * h) * q_norm)) /
+                           (T(-2) * dt * C_f / (h * h) * (q_norm / qx));
+                  if (fabs(temp) > T(5) * h * sqrt(h * g)) {
+                    qx = T(2) * temp - qx;
+                    if (qx * temp <= T(0)) qx = T(0);
+                  } else {
+                    qx = temp;
+                  }
+                }
+                if (fabs(qy) > T(1.0e-10)) {
+                  T temp = (T(1) - sqrt(T(1) + (T(4) * dt * C_f) / (h * h) * q_norm)) /
+                           (T(-2) * dt * C_f / (h * h) * (q_norm / qy));
+                  if (fabs(temp) > T(5) * h * sqrt(h * g)) {
+                    qy = T(2) * temp - qy;
+                    if (qy * temp <= T(0)) qy = T(0);
+                  } else {
+                    qy = temp;
+                  }
                 }
               }
             }
-          } else {
-            const T C_f = g * n * n * pow(h, T(-1.0 / 3.0));
-            const T q_norm = sqrt(qx * qx + qy * qy);
-            if (n > T(0)) {
-              if (fabs(qx) > T(1.0e-10)) {
-                T temp = (T(1) - sqrt(T(1) + (T(4) * dt * C_f) / (h * h) * q_norm)) /
-                         (T(-2) * dt * C_f / (h * h) * (q_norm / qx));
-                if (fabs(temp) > T(5) * h * sqrt(h * g)) {
-                  qx = T(2) * temp - qx;
-                  if (qx * temp <= T(0)) qx = T(0);
-                } else {
-                  qx = temp;
-                }
-              }
-              if (fabs(qy) > T(1.0e-10)) {
-                T temp = (T(1) - sqrt(T(1) + (T(4) * dt * C_f) / (h * h) * q_norm)) /
-                         (T(-2) * dt * C_f / (h * h) * (q_norm / qy));
-                if (fabs(temp) > T(5) * h * sqrt(h * g)) {
-                  qy = T(2) * temp - qy;
-                  if (qy * temp <= T(0)) qy = T(0);
-                } else {
-                  qy = temp;
-                }
-              }
-            }
           }
+          const size_t go = (size_t)(ry + HB_PAD_Y) * P + (rx + HB_PAD_X);
+          hout[go] = h;
+          qxout[go] = qx;
+          qyout[go] = qy;
+          hmaxg[go] = fmax(h, s.hmax[i * kTW + j]);
+          if (h > hs) {
+            // CFL speed (HC/timeControl_Kernel.cu:186-189)
+            const T sp = FAST ? sgh + fmax(fabs(qx), fabs(qy)) * ih
+                              : sgh + fmax(fabs(qx), fabs(qy)) / h;
+            smax_t = fmax(smax_t, sp);
+          } else {
+            any_dry = 1;
+          }
+          vol_t += h;
         }
-        const size_t go = (size_t)(ry + HB_PAD_Y) * P + (rx + HB_PAD_X);
-        hout[go] = h;
-        qxout[go] = qx;
-        qyout[go] = qy;
-        hmaxg[go] = fmax(h, s.hmax[i * kTW + j]);
-        if (h > hs) {
-          // CFL speed (HC/timeControl_Kernel.cu:186-189)
-          const T sp = FAST ? sgh + fmax(fabs(qx), fabs(qy)) * ih
-                            : sgh + fmax(fabs(qx), fabs(qy)) / h;
-          smax_t = fmax(smax_t, sp);
-        } else {
-          any_dry = 1;
+        // slide the column window down one row
+        nf = sf;
+        cN = cC; kN = kC;
+        cC = cS; kC = kS;
+        syC = syS;
+        if (i + 1 < r0 + R) {
+          cS = V.cell(i + 2, j);
+          kS = V.code(i + 2, j);
+          const Cell<T> cSS = V.cell(i + 3, j);
+          const uint8_t kSS = V.code(i + 3, j);
+          syS = slope_of(cS, cSS, valid(kSS), cC, valid(kC));
         }
-        vol_t += h;
       }
-      // slide the column window down one row
-      nf = sf;
-      cN = cC; kN = kC;
-      cC = cS; kC = kS;
-      syC = syS;
-      if (i + 1 < r0 + R) {
-        cS = V.cell(i + 2, j);
-        kS = V.code(i + 2, j);
-        const Cell<T> cSS = V.cell(i + 3, j);
-        const uint8_t kSS = V.code(i + 3, j);
-        syS = slope_of(cS, cSS, is_valid(kSS), cC, is_valid(kC));
-      }
-    }
+
+    };
+    if (allv)
+      rows(BoolTag<true>{});
+    else
+      rows(BoolTag<false>{});
 
     // --- tile partials and the instance's last-tile finalize
     double vol = warp_sum((double)vol_t);
