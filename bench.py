@@ -216,7 +216,8 @@ def run_ours(args) -> None:
         d = S.urban_catchment(args.cells, dx=2.0, seed=0, n_rows=args.cells * max(world, 1))
         if world > 1:
             strips = DistributedStrips(catchment_from(d), rank, world, dtype=torch.float32,
-                                       tile=tuple(args.tile), device=dev, minb=args.minb)
+                                       tile=tuple(args.tile), device=dev, minb=args.minb,
+                                       peer=args.peer)
         else:
             strips = StripSolver(catchment_from(d), 2, dtype=torch.float32,
                                  tile=tuple(args.tile), device=dev, minb=args.minb)
@@ -675,6 +676,9 @@ def main() -> None:
     ap.add_argument("--ensemble-steps", type=int, default=20)
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false")
     ap.add_argument("--no-coupled", dest="coupled", action="store_false")
+    ap.add_argument("--peer", action="store_true",
+                    help="with --strips on N > 1 GPUs: the step kernel writes the neighbour "
+                         "ranks' halo rows through CUDA IPC mappings (one node)")
     ap.add_argument("--strips", action="store_true",
                     help="one catchment split in row strips over the GPUs (halo exchange) "
                          "instead of independent replicas")

@@ -1324,6 +1324,10 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
       // build, in which both branches vanish)
       const bool infil = SOURCES && in.cum != nullptr;
       const bool stations = SOURCES && in.rain_station != nullptr;
+      // row strips: does this tile hold rows whose new state also goes to a
+      // neighbour strip's halo rows?
+      const bool fwd_tile = (y0 < HB_PAD_Y && in.halo_up[0] != nullptr) ||
+                            (y0 + TY > in.rows - HB_PAD_Y && in.halo_down[0] != nullptr);
 
   #pragma unroll 1
       for (int i = r0; i < r0 + R; ++i) {
@@ -1496,6 +1500,21 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
           hout[go] = h;
           qxout[go] = qx;
           qyout[go] = qy;
+          if (fwd_tile) {
+            // into the neighbour's halo row of the same output buffer (plain
+            // stores; the neighbour's arrays may be on a peer GPU)
+            const int ob = 1 - cur;
+            auto fwd = [&](void *const *dst, int row) {
+              const size_t gh = (size_t)row * P + (rx + HB_PAD_X);
+              ((T *)dst[ob])[gh] = h;
+              ((T *)dst[2 + ob])[gh] = qx;
+              ((T *)dst[4 + ob])[gh] = qy;
+            };
+            if (ry < HB_PAD_Y && in.halo_up[0] != nullptr)
+              fwd(in.halo_up, in.halo_up_rows + HB_PAD_Y + ry);
+            if (ry >= in.rows - HB_PAD_Y && in.halo_down[0] != nullptr)
+              fwd(in.halo_down, ry - in.rows + HB_PAD_Y);
+          }
           hmaxg[go] = fmax(h, s.hmax[i * kTW + j]);
           if (h > hs) {
             // CFL speed (HC/timeControl_Kernel.cu:186-189)
@@ -1810,6 +1829,10 @@ int prepare_impl(const hb_fused_batch *b, cudaStream_t st, CUtensorMap *host_map
       if (src && !uses_rows_kernel(b))
         return set_error(HB_ERR_ARG,
                          "hb_fused_prepare: infiltration and station rain need the rows kernel");
+      if (b->instances_host[i].halo_up[0] || b->instances_host[i].halo_down[0]) {
+        if (!uses_rows_kernel(b))
+          return set_error(HB_ERR_ARG, "hb_fused_prepare: halo forwarding needs the rows kernel");
+      }
       if (src && !(b->flags & HB_FLAG_SOURCES))
         return set_error(HB_ERR_ARG, "hb_fused_prepare: instance %d has infiltration or "
                                      "station rain; set HB_FLAG_SOURCES", i);

@@ -67,6 +67,7 @@ class HbInstance(ctypes.Structure):
         ("dtheta", c_dbl * HB_MAX_ZONES),
         ("rain_station", c_vp), ("station_rate", c_vp), ("station_cells", c_vp),
         ("n_stations", c_i32), ("pad2", c_i32),
+        ("halo_up", c_vp * 6), ("halo_down", c_vp * 6), ("halo_up_rows", c_i32), ("pad3", c_i32),
     ]
 
 

@@ -22,6 +22,15 @@ Every face is evaluated from the same inputs as in the undivided run and the
 clock sees the same global speed, so the strips reproduce the single-domain
 result bit for bit.  Volumes and rain totals are per strip (sum them).
 Each strip must have at least three rows.
+
+Halo forwarding (the default for StripSolver, `peer=True` for
+DistributedStrips) folds step 1 into step 2: the step kernel stores the new
+state of each strip's first and last two rows also into the neighbour's halo
+rows of the same output buffer (hb_instance.halo_up / halo_down), which no
+kernel reads during that step.  Across ranks the neighbour's arrays are mapped
+with CUDA IPC, the stores are plain peer stores, and the clock all_reduce that
+follows every step orders them before the neighbour's next step.  One exchange
+at start-up fills the halos of the initial state.
 """
 from __future__ import annotations
 
@@ -105,12 +114,34 @@ def _static_halos(fs: FusedSolver, k: int, c: Catchment, a: int, b: int) -> None
             ins.z[pr].copy_(torch.as_tensor(zrow, dtype=fs.dtype, device=fs.device))
 
 
+def _state_arrays(ins) -> list[torch.Tensor]:
+    """[h0, h1, qx0, qx1, qy0, qy1] of one instance (the halo_* order)."""
+    return [ins.h[0], ins.h[1], ins.qx[0], ins.qx[1], ins.qy[0], ins.qy[1]]
+
+
+def _link(fs: FusedSolver, k: int, up: Sequence[int] | None, up_rows: int,
+          down: Sequence[int] | None) -> None:
+    """Set instance k's halo forwarding targets (device addresses of the
+    neighbours' six state arrays, or None) in the host records."""
+    r = fs._recs_host[k]
+    for j in range(6):
+        r.halo_up[j] = up[j] if up is not None else None
+        r.halo_down[j] = down[j] if down is not None else None
+    r.halo_up_rows = up_rows if up is not None else 0
+
+
+def _upload_records(fs: FusedSolver) -> None:
+    fs.records.copy_(torch.frombuffer(bytearray(fs._recs_host), dtype=torch.uint8))
+
+
 class StripSolver:
     """A catchment split into `parts` row strips, all on one device, advanced
-    with FusedSolver steps, halo copies and hb_fused_finish."""
+    with FusedSolver steps and hb_fused_finish.  forward_halos (default): the
+    step kernel writes the neighbours' halo rows; False: a halo copy before
+    every step."""
 
     def __init__(self, c: Catchment, parts: int, dtype=torch.float32, device="cuda",
-                 **solver_kw):
+                 forward_halos: bool = True, **solver_kw):
         mask = np.asarray(c.mask)
         self.ranges = split_rows(mask.shape[0], parts)
         self.catchment = c
@@ -124,11 +155,22 @@ class StripSolver:
             bug = (gbug[0] - a, gbug[1]) if inside else (-1, -1)
             self.fs.inst[k].bug = bug
             self.fs._recs_host[k].bug_y, self.fs._recs_host[k].bug_x = bug
-        self.fs.records.copy_(torch.frombuffer(bytearray(self.fs._recs_host), dtype=torch.uint8))
+        self.forward_halos = forward_halos
+        if forward_halos:
+            inst = self.fs.inst
+            ptrs = [[t.data_ptr() for t in _state_arrays(ins)] for ins in inst]
+            if any(ins.pitch != inst[0].pitch for ins in inst):
+                raise ValueError("strips of one catchment share the row pitch")
+            for k in range(len(inst)):
+                _link(self.fs, k, ptrs[k - 1] if k > 0 else None,
+                      inst[k - 1].rows if k > 0 else 0,
+                      ptrs[k + 1] if k + 1 < len(inst) else None)
+        _upload_records(self.fs)
         self.fs.set_external_dt(True)
         self._ext_off = _lib.HbCtrl.ext.offset // 8
         self._cdbl = self.fs._ctrl_size // 8
-        self._cur = 0
+        self._cur = self.fs.controls()[0].cur
+        self.exchange()  # halos of the initial state
 
     def exchange(self) -> None:
         """Copy every strip's two edge rows of h, qx, qy into its neighbours' halos."""
@@ -150,7 +192,8 @@ class StripSolver:
         L = _lib.lib()
         n = len(self.fs.inst)
         for _ in range(nsteps):
-            self.exchange()
+            if not self.forward_halos:
+                self.exchange()
             self.fs.step(1)
             g = self._ext().amax(dim=0, keepdim=True).expand(n, 2).contiguous()
             with torch.cuda.device(self.device):
@@ -170,10 +213,13 @@ class StripSolver:
 class DistributedStrips:
     """This rank's strip of a catchment split over `world` ranks of an
     initialised torch.distributed process group (NCCL on GPUs; the exchange
-    and reduction also run with gloo on CPU tensors)."""
+    and reduction also run with gloo on CPU tensors).  peer=True: the
+    neighbours' state arrays are mapped with CUDA IPC (ranks on one node) and
+    the step kernel writes their halo rows; otherwise a halo exchange before
+    every step."""
 
     def __init__(self, c: Catchment, rank: int, world: int, dtype=torch.float32,
-                 device="cuda", **solver_kw):
+                 device="cuda", peer: bool = False, **solver_kw):
         mask = np.asarray(c.mask)
         self.rank, self.world = rank, world
         self.ranges = split_rows(mask.shape[0], world)
@@ -185,10 +231,38 @@ class DistributedStrips:
         bug = (gbug[0] - a, gbug[1]) if a <= gbug[0] < b else (-1, -1)
         self.fs.inst[0].bug = bug
         self.fs._recs_host[0].bug_y, self.fs._recs_host[0].bug_x = bug
-        self.fs.records.copy_(torch.frombuffer(bytearray(self.fs._recs_host), dtype=torch.uint8))
+        self.peer = peer
+        self._peer_arrays: list[torch.Tensor] = []  # keeps the IPC mappings open
+        if peer:
+            self._map_neighbours()
+        _upload_records(self.fs)
         self.fs.set_external_dt(True)
         self._ext_off = _lib.HbCtrl.ext.offset // 8
-        self._cur = 0
+        self._cur = self.fs.controls()[0].cur
+        self.exchange()  # halos of the initial state
+
+    def _map_neighbours(self) -> None:
+        """CUDA IPC handles of every rank's state arrays go round the group;
+        this rank opens its neighbours' and points its halo forwarding at them."""
+        import torch.distributed as dist
+        from torch.multiprocessing.reductions import reduce_tensor
+
+        ins = self.fs.inst[0]
+        mine = ([reduce_tensor(t) for t in _state_arrays(ins)], ins.rows, ins.pitch)
+        every = [None] * self.world
+        dist.all_gather_object(every, mine)
+        ptr = {}
+        for nb in (self.rank - 1, self.rank + 1):
+            if 0 <= nb < self.world:
+                handles, rows, pitch = every[nb]
+                if pitch != ins.pitch:
+                    raise ValueError("strips of one catchment share the row pitch")
+                ts = [fn(*args) for fn, args in handles]
+                self._peer_arrays += ts
+                ptr[nb] = ([t.data_ptr() for t in ts], rows)
+        up, down = ptr.get(self.rank - 1), ptr.get(self.rank + 1)
+        _link(self.fs, 0, up[0] if up else None, up[1] if up else 0, down[0] if down else None)
+        dist.barrier()
 
     def exchange(self) -> None:
         ins = self.fs.inst[0]
@@ -200,10 +274,16 @@ class DistributedStrips:
 
         L = _lib.lib()
         for _ in range(nsteps):
-            self.exchange()
+            if not self.peer:
+                self.exchange()
             self.fs.step(1)
             ext = self.fs.ctrl.view(torch.float64)[self._ext_off:self._ext_off + 2].clone()
-            dist.all_reduce(ext, op=dist.ReduceOp.MAX)
+            if dist.get_backend() == "gloo":  # host staging (gloo ranks sharing a device)
+                host = ext.cpu()
+                dist.all_reduce(host, op=dist.ReduceOp.MAX)
+                ext = host.to(self.device)
+            else:
+                dist.all_reduce(ext, op=dist.ReduceOp.MAX)
             _lib.check(L.hb_fused_finish(ctypes.byref(self.fs.batch), ext.data_ptr(),
                                          self.fs._stream()), "hb_fused_finish")
             self._cur = 1 - self._cur
@@ -218,6 +298,14 @@ def exchange_halos(fields: Sequence[torch.Tensor], rows: int, rank: int, world: 
     import torch.distributed as dist
 
     PY = HALO
+    if dist.get_backend() == "gloo" and fields and fields[0].is_cuda:
+        # gloo sends host tensors: stage the edge rows through host memory
+        host = [F.cpu() for F in fields]
+        exchange_halos(host, rows, rank, world)
+        for F, H in zip(fields, host):
+            F[0:PY].copy_(H[0:PY])
+            F[PY + rows:PY + rows + PY].copy_(H[PY + rows:PY + rows + PY])
+        return
     ops, recvs = [], []
     for F in fields:
         if rank > 0:

@@ -128,6 +128,20 @@ typedef struct hb_instance {
   const double *station_cells; /* [n_stations] valid cells per station */
   int32_t n_stations;
   int32_t pad2;
+  /* optional halo forwarding between row strips of one catchment (no
+   * reference counterpart; replaces the halo exchange of
+   * HP/Parallel_SWE_CUDA.py).  The new h, qx, qy of this strip's first
+   * HB_PAD_Y rows are also stored into the bottom halo rows of the strip
+   * above (halo_up), and those of its last HB_PAD_Y rows into the top halo
+   * rows of the strip below (halo_down), in the output buffer of the step.
+   * Each side lists [h0, h1, qx0, qx1, qy0, qy1] of the neighbour (same
+   * columns and pitch as this strip); NULL halo_*[0]: no neighbour on that
+   * side.  The neighbour's arrays may be a peer GPU's memory (plain stores).
+   * Rows kernel only. */
+  void *halo_up[6];
+  void *halo_down[6];
+  int32_t halo_up_rows;      /* rows of the strip above */
+  int32_t pad3;
 } hb_instance;
 
 /* Launch record (host memory). */

@@ -92,7 +92,10 @@ def test_halo_exchange_and_clock_reduction_gloo():
 @pytest.mark.gpu
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
 @pytest.mark.parametrize("parts", [2, 3])
-def test_strips_reproduce_the_undivided_run(cuda, dtype, parts):
+@pytest.mark.parametrize("forward", [True, False])
+def test_strips_reproduce_the_undivided_run(cuda, dtype, parts, forward):
+    """forward: the step kernel writes the neighbours' halo rows; otherwise a
+    halo copy before every step."""
     from hipims_b200 import scenarios as S
     from hipims_b200.fused import FusedSolver
     from hipims_b200.strips import StripSolver
@@ -100,7 +103,7 @@ def test_strips_reproduce_the_undivided_run(cuda, dtype, parts):
     d = S.urban_catchment(192, dx=2.0, seed=8, rain_mm_h=120.0)
     c = S.catchment_from(d)
     one = FusedSolver(c, dtype=dtype, device=cuda)
-    st = StripSolver(c, parts, dtype=dtype, device=cuda)
+    st = StripSolver(c, parts, dtype=dtype, device=cuda, forward_halos=forward)
     for _ in range(3):
         one.step(20)
         st.step(20)
@@ -112,3 +115,64 @@ def test_strips_reproduce_the_undivided_run(cuda, dtype, parts):
             assert (cs.t, cs.dt, cs.step) == (c1.t, c1.dt, c1.step)
     vol = sum(cs.volume for cs in st.controls())
     assert vol == pytest.approx(one.controls()[0].volume, rel=1e-12)
+
+
+def _peer_rank_main(rank, world, port, q):
+    """One strip per process, both on GPU 0, gloo for the host-side
+    collectives; the step kernels write each other's halo rows through CUDA
+    IPC mappings.  No kernel waits on another: the clock all_reduce between
+    steps orders them."""
+    import torch.distributed as dist
+
+    from hipims_b200 import scenarios as S
+    from hipims_b200.strips import DistributedStrips
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        dev = torch.device("cuda", 0)
+        d = S.urban_catchment(160, dx=2.0, seed=11, rain_mm_h=120.0)
+        ds = DistributedStrips(S.catchment_from(d), rank, world, dtype=torch.float32,
+                               device=dev, peer=True)
+        ds.step(30)
+        torch.cuda.synchronize(dev)
+        st = ds.fs.state(0)
+        c = ds.fs.controls()[0]
+        q.put((rank, {f: st[f].cpu().numpy().copy() for f in ("h", "qx", "qy", "h_max")},
+               (c.t, c.dt, c.step)))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_peer_strips_on_one_device_reproduce_the_undivided_run(cuda):
+    from hipims_b200 import scenarios as S
+    from hipims_b200.fused import FusedSolver
+
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_peer_rank_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = {}
+    for _ in range(world):
+        rank, fields, clock = q.get(timeout=300)
+        res[rank] = (fields, clock)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    d = S.urban_catchment(160, dx=2.0, seed=11, rain_mm_h=120.0)
+    one = FusedSolver(S.catchment_from(d), dtype=torch.float32, device=cuda)
+    one.step(30)
+    want = one.state(0)
+    c1 = one.controls()[0]
+    for f in ("h", "qx", "qy", "h_max"):
+        got = np.concatenate([res[r][0][f] for r in range(world)], axis=0)
+        np.testing.assert_array_equal(got, want[f].cpu().numpy(), err_msg=f)
+    for r in range(world):
+        assert res[r][1] == (c1.t, c1.dt, c1.step)
