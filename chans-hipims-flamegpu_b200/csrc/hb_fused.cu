@@ -513,11 +513,24 @@ __device__ void close_group(const hb_instance &in, int ii, const TilePartial *ti
 template <typename T>
 __global__ void __launch_bounds__(kNT)
 finish_kernel(const hb_instance *__restrict__ insts, BcTable *__restrict__ bct,
-              const double *__restrict__ ext) {
+              const double *__restrict__ ext, int n_instances) {
   const hb_instance &in = insts[blockIdx.x];
   if (in.ctrl->halted) return;
-  advance_clock<T, kNT>(in, blockIdx.x, bct, ext[2 * blockIdx.x],
-                        ext[2 * blockIdx.x + 1] != 0.0 ? 1 : 0, in.ctrl);
+  double sm, dry;
+  if (ext) {
+    sm = ext[2 * blockIdx.x];
+    dry = ext[2 * blockIdx.x + 1];
+  } else {
+    // the batch's instances are the strips of one catchment: the maximum of
+    // what every instance published (order-independent)
+    sm = 0.0;
+    dry = 0.0;
+    for (int k = 0; k < n_instances; k++) {
+      sm = fmax(sm, __ldcg(&insts[k].ctrl->ext[0]));
+      dry = fmax(dry, __ldcg(&insts[k].ctrl->ext[1]));
+    }
+  }
+  advance_clock<T, kNT>(in, blockIdx.x, bct, sm, dry != 0.0 ? 1 : 0, in.ctrl);
 }
 
 // Workspace layout (each part 256-byte aligned): [n_tiles] TilePartial,
@@ -1877,14 +1890,14 @@ extern "C" int hb_fused_prepare(const hb_fused_batch *b, void *stream) {
 }
 
 extern "C" int hb_fused_finish(const hb_fused_batch *b, const double *ext, void *stream) {
-  if (!b || !b->instances || !b->workspace || b->n_instances <= 0 || !ext)
-    return set_error(HB_ERR_ARG, "hb_fused_finish: bad batch record or null ext");
+  if (!b || !b->instances || !b->workspace || b->n_instances <= 0)
+    return set_error(HB_ERR_ARG, "hb_fused_finish: bad batch record");
   BcTable *bct = reinterpret_cast<BcTable *>((char *)b->workspace + ws_bct_offset(b));
   auto st = as_stream(stream);
   if (b->dtype == HB_F64)
-    finish_kernel<double><<<b->n_instances, kNT, 0, st>>>(b->instances, bct, ext);
+    finish_kernel<double><<<b->n_instances, kNT, 0, st>>>(b->instances, bct, ext, b->n_instances);
   else if (b->dtype == HB_F32)
-    finish_kernel<float><<<b->n_instances, kNT, 0, st>>>(b->instances, bct, ext);
+    finish_kernel<float><<<b->n_instances, kNT, 0, st>>>(b->instances, bct, ext, b->n_instances);
   else
     return set_error(HB_ERR_ARG, "hb_fused_finish: bad dtype %d", b->dtype);
   return check_launch("hb_fused_finish");

@@ -14,9 +14,10 @@ below the raster, so the step kernel runs unchanged; per time step:
      on CPU tensors, across ranks);
   2. the fused step on every strip, with the control block's external_dt
      set: the step publishes its largest wave speed and any-dry flag;
-  3. the maximum of those over all strips (a torch max on one GPU,
-     all_reduce(MAX) across ranks) feeds hb_fused_finish, which advances
-     every strip's clock identically (CFL dt, 10x cap, export clip).
+  3. the maximum of those over all strips (taken by hb_fused_finish itself
+     on one GPU, by all_reduce(MAX) across ranks) feeds hb_fused_finish,
+     which advances every strip's clock identically (CFL dt, 10x cap, export
+     clip).
 
 Every face is evaluated from the same inputs as in the undivided run and the
 clock sees the same global speed, so the strips reproduce the single-domain
@@ -167,8 +168,6 @@ class StripSolver:
                       ptrs[k + 1] if k + 1 < len(inst) else None)
         _upload_records(self.fs)
         self.fs.set_external_dt(True)
-        self._ext_off = _lib.HbCtrl.ext.offset // 8
-        self._cdbl = self.fs._ctrl_size // 8
         self._cur = self.fs.controls()[0].cur
         self.exchange()  # halos of the initial state
 
@@ -184,20 +183,15 @@ class StripSolver:
                 D[0:PY].copy_(U[PY + ru - PY:PY + ru])      # up's last rows -> dn's top halo
                 U[PY + ru:PY + ru + PY].copy_(D[PY:2 * PY])  # dn's first rows -> up's bottom halo
 
-    def _ext(self) -> torch.Tensor:
-        c = self.fs.ctrl.view(torch.float64).view(len(self.fs.inst), self._cdbl)
-        return c[:, self._ext_off:self._ext_off + 2]
-
     def step(self, nsteps: int = 1) -> None:
         L = _lib.lib()
-        n = len(self.fs.inst)
         for _ in range(nsteps):
             if not self.forward_halos:
                 self.exchange()
             self.fs.step(1)
-            g = self._ext().amax(dim=0, keepdim=True).expand(n, 2).contiguous()
+            # NULL ext: the finish kernel takes the maximum over the strips itself
             with torch.cuda.device(self.device):
-                _lib.check(L.hb_fused_finish(ctypes.byref(self.fs.batch), g.data_ptr(),
+                _lib.check(L.hb_fused_finish(ctypes.byref(self.fs.batch), None,
                                              self.fs._stream()), "hb_fused_finish")
             self._cur = 1 - self._cur
 

@@ -134,7 +134,9 @@ int hb_fused_step(const struct hb_fused_batch *batch, int nsteps, void *stream);
  * counterpart in the reference; one catchment split into row strips over
  * several instances or GPUs): ext = device [n_instances][2], the largest wave
  * speed and the any-dry flag of each instance's whole catchment (the maximum
- * of hb_ctrl.ext over its strips).  Applies HP/SWE_CUDA.py:818-831 (CFL dt,
+ * of hb_ctrl.ext over its strips).  ext = NULL: the batch's instances are
+ * all the strips of one catchment, and every instance uses the maximum of
+ * hb_ctrl.ext over the batch.  Applies HP/SWE_CUDA.py:818-831 (CFL dt,
  * 10x cap, export clip, t += dt) and sets the next step's rain rate and
  * boundary values.  One step, then this, per time step. */
 int hb_fused_finish(const struct hb_fused_batch *batch, const double *ext, void *stream);
