@@ -375,15 +375,15 @@ def run_ours(args) -> None:
 
 
 def strip_config(args, world: int) -> dict:
-    if not args.strips:
-        return {}
     if world > 1:
+        halo = ("halo rows written by the step kernel through CUDA IPC peer mappings"
+                if args.peer else "NCCL halo exchange (2 rows of h, qx, qy each way)")
         return {"decomposition": f"one {args.cells * world}x{args.cells} catchment in {world} "
-                                 f"row strips, one per GPU: NCCL halo exchange (2 rows of h, "
-                                 f"qx, qy each way) and all_reduce(MAX) of the clock inputs "
-                                 f"per step", "parallelism": f"strips x{world}"}
+                                 f"row strips, one per GPU: {halo} and all_reduce(MAX) of the "
+                                 f"clock inputs per step", "parallelism": f"strips x{world}"}
     return {"decomposition": f"one {args.cells}x{args.cells} catchment in 2 row strips on one "
-                             f"GPU (device halo copies, clock reduced by torch max)"}
+                             f"GPU (halo rows written by the step kernel, clock inputs reduced "
+                             f"by hb_fused_finish)"}
 
 
 def plain_fp64_rate(d: dict, dev, steps: int = 5, reference_kernels: bool = True) -> dict:
