@@ -165,6 +165,30 @@ def test_fused_batch_equals_single_runs(cuda):
         assert fb.controls()[k].t == f1.controls()[0].t
 
 
+def test_fused_persistent_grid_equals_one_block_per_tile(cuda):
+    """A few CTAs looping over every tile of a batch (grid_blocks > 0) against
+    the default of one CTA per tile: the per-tile partials and the fixed-order
+    group sums make fields, clocks and volumes identical, bit for bit.  The
+    400 x 400 catchment has 169 tiles, so two reduction groups."""
+    from hipims_b200 import scenarios as S
+    from hipims_b200.fused import FusedSolver
+
+    ds = [S.urban_catchment(n, seed=k + 20, rain_mm_h=100.0) for k, n in enumerate((400, 70, 130))]
+    cs = [catchment(d) for d in ds]
+    a = FusedSolver(cs, dtype=torch.float32, device=cuda, tile=(32, 32))
+    b = FusedSolver(cs, dtype=torch.float32, device=cuda, tile=(32, 32), grid_blocks=7)
+    a.step(40)
+    b.step(40)
+    for k in range(len(cs)):
+        x, y = a.compacted(k), b.compacted(k)
+        for f in ("h", "qx", "qy", "h_max"):
+            np.testing.assert_array_equal(x[f], y[f])
+        ca, cb = a.controls()[k], b.controls()[k]
+        assert (ca.t, ca.dt, ca.step) == (cb.t, cb.dt, cb.step)
+        assert (ca.volume, ca.outflow_volume, ca.rain_volume) == \
+            (cb.volume, cb.outflow_volume, cb.rain_volume)
+
+
 def test_fused_graph_replay_equals_eager(cuda):
     from hipims_b200 import scenarios as S
     from hipims_b200.fused import FusedSolver
