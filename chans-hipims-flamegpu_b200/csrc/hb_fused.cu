@@ -32,6 +32,7 @@
 
 #include <algorithm>
 #include <mutex>
+#include <unordered_map>
 #include <vector>
 
 #include "hb_common.cuh"
@@ -535,7 +536,9 @@ finish_kernel(const hb_instance *__restrict__ insts, BcTable *__restrict__ bct,
 
 // Workspace layout (each part 256-byte aligned): [n_tiles] TilePartial,
 // [n_groups] TilePartial (sums of groups of kGroupTiles tiles), [n_groups]
-// unsigned group counters, [n_instances] BcTable, then
+// unsigned group counters, [n_tiles] int32 tile order (rows kernel: general
+// tiles, then all-valid tiles), [2] int32 counts of the two, [n_tiles] uint8
+// all-valid flags, [n_instances] BcTable, then
 // [n_instances][kMapsPerInstance] CUtensorMap.  Instance i's groups start at
 // tile_begin / kGroupTiles + i, which never overlaps instance i + 1's.
 inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -546,8 +549,15 @@ inline int ws_n_groups(const hb_fused_batch *b) {
 inline size_t ws_gcount_offset(const hb_fused_batch *b) {
   return ws_partials_bytes(b->n_tiles) + align256((size_t)ws_n_groups(b) * sizeof(TilePartial));
 }
-inline size_t ws_bct_offset(const hb_fused_batch *b) {
+inline size_t ws_order_offset(const hb_fused_batch *b) {
   return ws_gcount_offset(b) + align256((size_t)ws_n_groups(b) * sizeof(unsigned));
+}
+inline size_t ws_counts_offset(const hb_fused_batch *b) {
+  return ws_order_offset(b) + align256((size_t)b->n_tiles * sizeof(int32_t));
+}
+inline size_t ws_flags_offset(const hb_fused_batch *b) { return ws_counts_offset(b) + 256; }
+inline size_t ws_bct_offset(const hb_fused_batch *b) {
+  return ws_flags_offset(b) + align256((size_t)b->n_tiles);
 }
 inline size_t ws_maps_offset(const hb_fused_batch *b) {
   return align256(ws_bct_offset(b) + (size_t)b->n_instances * sizeof(BcTable));
@@ -1149,12 +1159,22 @@ __device__ __forceinline__ FaceOut<T> face_any(const RowsSmem<T, TY> &s, const C
   return o;
 }
 
-template <typename T, int TY, bool FAST, int MINB, bool SOURCES = false>
+// PATH 0: the general row loop, over the tiles that prepare classified as
+// touching no-data cells or the cell-0 rule's cell; PATH 1: the all-valid row
+// loop (every validity test a compile-time true), over the other tiles.  The
+// two paths are separate kernels so that each gets its own register
+// allocation (the general path's ghost faces and selects cost the all-valid
+// tiles registers, spills and about 9 % of their time when they share one).
+// order[0, counts[0]) are the general tiles, order[counts[0], counts[0] +
+// counts[1]) the all-valid ones.
+template <typename T, int TY, bool FAST, int MINB, bool SOURCES, int PATH>
 __global__ void __launch_bounds__(kRowsNT, MINB)
 rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restrict__ tile_inst,
-                 int n_tiles, TilePartial *__restrict__ partials, TilePartial *__restrict__ gparts,
+                 const int32_t *__restrict__ order, const int32_t *__restrict__ counts,
+                 TilePartial *__restrict__ partials, TilePartial *__restrict__ gparts,
                  unsigned *__restrict__ gcount, BcTable *__restrict__ bct,
                  const CUtensorMap *__restrict__ maps) {
+  constexpr bool kAllValid = PATH == 1;
   using S = RowsSmem<T, TY>;
   constexpr int R = S::R;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -1169,7 +1189,10 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
   __syncthreads();
   unsigned phase = 0;
 
-  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+  const int n_list = counts[PATH];
+  const int32_t *list = order + (kAllValid ? counts[0] : 0);
+  for (int k = blockIdx.x; k < n_list; k += gridDim.x) {
+    const int tile = list[k];
     const int ii = tile_inst[tile];
     const hb_instance &in = insts[ii];
     hb_ctrl *ctrl = in.ctrl;
@@ -1248,22 +1271,7 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
         if (dyb != 1 || dxb != 1) s.f[3][V.fi(i, j)] += s.ddatum[dyb * 3 + dxb];
       }
     }
-    // All-valid tile: every staged code of rows -2..TY+1, columns -4..35 is a
-    // valid cell and the cell-0 rule's cell is out of reach.  The row loop
-    // then runs with each validity test a compile-time true: the same
-    // arithmetic without no-data selects, ghost-face branches or
-    // boundary-outflow terms.
-    bool ok = !(bug_y >= y0 - 2 && bug_y <= y0 + TY + 1 && bug_x >= x0 - 4 && bug_x <= x0 + 35);
-    {
-      constexpr unsigned kNoData4 = 0x01010101u * (unsigned)(HB_NODATA_CLASS << 4);
-      const unsigned *cw = reinterpret_cast<const unsigned *>(s.code);
-      // 10 words per staged code row: bytes 12..51 are columns -4..35
-      for (int k = tid; k < S::SH * 10; k += kRowsNT) {
-        const unsigned w4 = cw[(k / 10) * (kSWC / 4) + 3 + k % 10];
-        ok = ok && (__vcmpeq4(w4 & 0xF0F0F0F0u, kNoData4) == 0u);
-      }
-    }
-    const bool allv = __syncthreads_and(ok) != 0;
+    __syncthreads();
 
     const int r0 = w * R;
     // --- tile edges, all lanes busy: warp 0 evaluates the faces between
@@ -1275,7 +1283,7 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
         const uint8_t ca = V.code(i, 31), cb = V.code(i, 32);
         const Slope<T> sa = slope_of(a, V.cell(i, 30), is_valid(V.code(i, 30)), b, is_valid(cb));
         const Slope<T> sb = slope_of(b, a, is_valid(ca), V.cell(i, 33), is_valid(V.code(i, 33)));
-        const FaceOut<T> f = face_any<T, FAST, 0>(s, a, ca, b, cb, sa, sb, datum_tile);
+        const FaceOut<T> f = face_any<T, FAST, 0, TY, kAllValid>(s, a, ca, b, cb, sa, sb, datum_tile);
         s.xe[i][0] = f.fh;
         s.xe[i][1] = f.fx;
         s.xe[i][2] = f.fy;
@@ -1554,10 +1562,7 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
       }
 
     };
-    if (allv)
-      rows(BoolTag<true>{});
-    else
-      rows(BoolTag<false>{});
+    rows(BoolTag<kAllValid>{});
 
     // --- tile partials and the instance's last-tile finalize
     double vol = warp_sum((double)vol_t);
@@ -1684,38 +1689,181 @@ int launch_steps(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   return check_launch("hb_fused_step");
 }
 
+// ---------------------------------------------------------------------------
+// Tile classification (at prepare): a tile is all-valid when every staged
+// code of rows -2..TY+1, columns -4..35 is a valid cell and the cell-0 rule's
+// cell is out of its reach; the rows kernel runs those tiles in its all-valid
+// build and the others in its general build.
+// ---------------------------------------------------------------------------
+template <int TY>
+__global__ void __launch_bounds__(kRowsNT)
+classify_tiles_kernel(const hb_instance *__restrict__ insts, const int32_t *__restrict__ tile_inst,
+                      int n_tiles, uint8_t *__restrict__ flags) {
+  const int tile = blockIdx.x;
+  if (tile >= n_tiles) return;
+  const hb_instance &in = insts[tile_inst[tile]];
+  const int lt = tile - in.tile_begin;
+  const int tyi = lt / in.tiles_x, txi = lt - tyi * in.tiles_x;
+  const int y0 = tyi * TY, x0 = txi * kTW;
+  bool ok = !(in.bug_y >= y0 - 2 && in.bug_y <= y0 + TY + 1 && in.bug_x >= x0 - 4 &&
+              in.bug_x <= x0 + 35);
+  // raster row y is code row y + HB_PAD_Y, raster column x code column
+  // x + HB_CODE_PAD_X; the region lies inside the padded code array
+  constexpr int W = kTW + 8;
+  for (int k = threadIdx.x; k < (TY + 4) * W; k += kRowsNT) {
+    const int y = y0 - 2 + k / W, x = x0 - 4 + k % W;
+    const uint8_t c = in.code[(size_t)(y + HB_PAD_Y) * in.code_pitch + (x + HB_CODE_PAD_X)];
+    ok = ok && is_valid(c);
+  }
+  ok = __syncthreads_and(ok) != 0;
+  if (threadIdx.x == 0) flags[tile] = ok ? 1 : 0;
+}
+
+// Stable partition of the tiles by flag, one block: order = general tiles
+// (flag 0) in index order, then all-valid tiles (flag 1) in index order;
+// counts = {general, all-valid}.
+constexpr int kOrderNT = 1024;
+__global__ void __launch_bounds__(kOrderNT)
+order_tiles_kernel(const uint8_t *__restrict__ flags, int n, int32_t *__restrict__ order,
+                   int32_t *__restrict__ counts) {
+  __shared__ int s_g[kOrderNT / 32], s_a[kOrderNT / 32];
+  __shared__ int s_total, s_base[2];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  if (tid == 0) s_total = 0;
+  __syncthreads();
+  int cnt = 0;
+  for (int i = tid; i < n; i += kOrderNT) cnt += flags[i] == 0;
+  atomicAdd(&s_total, cnt);
+  __syncthreads();
+  if (tid == 0) {
+    s_base[0] = 0;
+    s_base[1] = s_total;
+  }
+  __syncthreads();
+  const unsigned below = (1u << lane) - 1u;
+  for (int c = 0; c < n; c += kOrderNT) {
+    const int i = c + tid;
+    const int f = i < n ? flags[i] : 2;
+    const unsigned bg = __ballot_sync(0xffffffffu, f == 0);
+    const unsigned ba = __ballot_sync(0xffffffffu, f == 1);
+    if (lane == 0) {
+      s_g[w] = __popc(bg);
+      s_a[w] = __popc(ba);
+    }
+    __syncthreads();
+    int og = 0, oa = 0;  // warps before this one
+    for (int q = 0; q < w; q++) {
+      og += s_g[q];
+      oa += s_a[q];
+    }
+    if (f == 0) order[s_base[0] + og + __popc(bg & below)] = i;
+    if (f == 1) order[s_base[1] + oa + __popc(ba & below)] = i;
+    __syncthreads();
+    if (tid == 0) {
+      int tg = 0, ta = 0;
+      for (int q = 0; q < kOrderNT / 32; q++) {
+        tg += s_g[q];
+        ta += s_a[q];
+      }
+      s_base[0] += tg;
+      s_base[1] += ta;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    counts[0] = s_total;
+    counts[1] = n - s_total;
+  }
+}
+
+// Per-device side stream (highest priority) and fork/join events for the
+// general-tile kernel, created by hb_fused_prepare (outside any capture) and
+// kept until exit.  The mutex keeps one fork/join sequence whole when several
+// host threads step batches on one device.
+constexpr int kMaxSideDevices = 64;
+struct SideRes {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+std::mutex g_side_mu;
+SideRes g_side[kMaxSideDevices];
+// counts of general tiles per prepared workspace (read back at prepare), so
+// that the general-tile kernel gets one CTA per tile; guarded by g_side_mu
+std::unordered_map<const void *, int> g_general_tiles;
+
+int side_setup() {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return set_error(HB_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxSideDevices)
+    return set_error(HB_ERR_LIMIT, "hb_fused_prepare: device %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_side_mu);
+  SideRes &r = g_side[dev];
+  if (r.stream) return HB_OK;
+  int lo = 0, hi = 0;
+  e = cudaDeviceGetStreamPriorityRange(&lo, &hi);
+  if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&r.stream, cudaStreamNonBlocking, hi);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r.fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r.join, cudaEventDisableTiming);
+  if (e != cudaSuccess) return set_error(HB_ERR_CUDA, "side stream setup: %s", cudaGetErrorString(e));
+  return HB_OK;
+}
+
 template <typename T, int TY, bool FAST = (sizeof(T) == 4), int MINB = 1, bool SOURCES = false>
 int launch_rows_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   using S = RowsSmem<T, TY>;
+  // the all-valid build needs fewer registers: one more resident CTA per SM
+  // where the general build is held to five
+  constexpr int MINB_A = (TY == 32 && MINB == 5) ? 6 : MINB;
+  auto *kg = rows_step_kernel<T, TY, FAST, MINB, SOURCES, 0>;
+  auto *ka = rows_step_kernel<T, TY, FAST, MINB_A, SOURCES, 1>;
   static std::once_flag once;
   static cudaError_t attr_err = cudaSuccess;
-  static int blocks_per_sm = 1;
-  std::call_once(once, [] {
-    attr_err = cudaFuncSetAttribute(rows_step_kernel<T, TY, FAST, MINB, SOURCES>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(S));
+  std::call_once(once, [&] {
+    attr_err = cudaFuncSetAttribute(kg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(S));
     if (attr_err == cudaSuccess)
-      attr_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &blocks_per_sm, rows_step_kernel<T, TY, FAST, MINB, SOURCES>, kRowsNT, sizeof(S));
-    if (blocks_per_sm < 1) blocks_per_sm = 1;
+      attr_err = cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)sizeof(S));
   });
   if (attr_err != cudaSuccess)
     return set_error(HB_ERR_CUDA, "fused step setup: %s", cudaGetErrorString(attr_err));
-  // one CTA per tile by default: the block scheduler starts the next tile as
-  // soon as a CTA retires, which balances tiles of uneven cost (boundary
-  // columns, wet fronts) better than a fixed share per resident CTA; a
-  // positive grid_blocks makes the CTAs loop over tiles instead
-  (void)blocks_per_sm;
-  int grid = b->grid_blocks > 0 ? b->grid_blocks : b->n_tiles;
-  if (grid > b->n_tiles) grid = b->n_tiles;
+  // One CTA per tile by default (the block scheduler starts the next tile as
+  // soon as a CTA retires, which balances tiles of uneven cost): the general
+  // tiles on the side stream, at the highest priority so that the slower
+  // tiles start first, the all-valid tiles on the caller's stream; both
+  // kernels run at once.  A positive grid_blocks makes every CTA loop over
+  // its kernel's tiles.
+  std::lock_guard<std::mutex> lock(g_side_mu);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxSideDevices ||
+      !g_side[dev].stream)
+    return set_error(HB_ERR_ARG, "hb_fused_step: run hb_fused_prepare on this device first");
+  const SideRes &sr = g_side[dev];
+  const int n = b->n_tiles;
+  int n_general = n;  // unknown workspace: CTAs beyond the general count exit at once
+  const auto it = g_general_tiles.find(b->workspace);
+  if (it != g_general_tiles.end()) n_general = std::max(it->second, 1);
+  const int grid_a = b->grid_blocks > 0 ? std::min(b->grid_blocks, n) : n;
+  const int grid_g = b->grid_blocks > 0 ? std::min(b->grid_blocks, n) : std::min(n_general, n);
   char *ws = reinterpret_cast<char *>(b->workspace);
   TilePartial *parts = reinterpret_cast<TilePartial *>(ws);
   TilePartial *gparts = reinterpret_cast<TilePartial *>(ws + ws_partials_bytes(b->n_tiles));
   unsigned *gcount = reinterpret_cast<unsigned *>(ws + ws_gcount_offset(b));
+  const int32_t *order = reinterpret_cast<const int32_t *>(ws + ws_order_offset(b));
+  const int32_t *counts = reinterpret_cast<const int32_t *>(ws + ws_counts_offset(b));
   BcTable *bct = reinterpret_cast<BcTable *>(ws + ws_bct_offset(b));
   const CUtensorMap *maps = reinterpret_cast<const CUtensorMap *>(ws + ws_maps_offset(b));
   for (int k = 0; k < nsteps; k++) {
-    rows_step_kernel<T, TY, FAST, MINB, SOURCES><<<grid, kRowsNT, sizeof(S), st>>>(
-        b->instances, b->tile_instance, b->n_tiles, parts, gparts, gcount, bct, maps);
+    cudaError_t e = cudaEventRecord(sr.fork, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(sr.stream, sr.fork, 0);
+    if (e != cudaSuccess) return set_error(HB_ERR_CUDA, "hb_fused_step fork: %s", cudaGetErrorString(e));
+    kg<<<grid_g, kRowsNT, sizeof(S), sr.stream>>>(b->instances, b->tile_instance, order, counts,
+                                                  parts, gparts, gcount, bct, maps);
+    ka<<<grid_a, kRowsNT, sizeof(S), st>>>(b->instances, b->tile_instance, order, counts, parts,
+                                           gparts, gcount, bct, maps);
+    e = cudaEventRecord(sr.join, sr.stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, sr.join, 0);
+    if (e != cudaSuccess) return set_error(HB_ERR_CUDA, "hb_fused_step join: %s", cudaGetErrorString(e));
   }
   return check_launch("hb_fused_step");
 }
@@ -1859,6 +2007,30 @@ int prepare_impl(const hb_fused_batch *b, cudaStream_t st, CUtensorMap *host_map
                                           (size_t)ws_n_groups(b) * sizeof(unsigned), st);
     if (e != cudaSuccess)
       return set_error(HB_ERR_CUDA, "hb_fused_prepare: %s", cudaGetErrorString(e));
+  }
+  if (uses_rows_kernel(b) && b->n_tiles > 0) {
+    // the side stream of the general tiles, and the tile classification
+    int rc = side_setup();
+    if (rc) return rc;
+    char *ws = reinterpret_cast<char *>(b->workspace);
+    uint8_t *flags = reinterpret_cast<uint8_t *>(ws + ws_flags_offset(b));
+    if (b->tile_y == 64)
+      classify_tiles_kernel<64><<<b->n_tiles, kRowsNT, 0, st>>>(b->instances, b->tile_instance,
+                                                                 b->n_tiles, flags);
+    else
+      classify_tiles_kernel<32><<<b->n_tiles, kRowsNT, 0, st>>>(b->instances, b->tile_instance,
+                                                                 b->n_tiles, flags);
+    order_tiles_kernel<<<1, kOrderNT, 0, st>>>(
+        flags, b->n_tiles, reinterpret_cast<int32_t *>(ws + ws_order_offset(b)),
+        reinterpret_cast<int32_t *>(ws + ws_counts_offset(b)));
+    int32_t counts[2] = {0, 0};
+    cudaError_t e = cudaMemcpyAsync(counts, ws + ws_counts_offset(b), sizeof(counts),
+                                    cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess)
+      return set_error(HB_ERR_CUDA, "hb_fused_prepare: tile classes: %s", cudaGetErrorString(e));
+    std::lock_guard<std::mutex> lock(g_side_mu);
+    g_general_tiles[b->workspace] = counts[0];
   }
   // blocks per instance for the volume sum: about 16 cells per thread of the
   // largest instance (the host copy of the records gives the sizes)
