@@ -1812,9 +1812,11 @@ int side_setup() {
 template <typename T, int TY, bool FAST = (sizeof(T) == 4), int MINB = 1, bool SOURCES = false>
 int launch_rows_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   using S = RowsSmem<T, TY>;
-  // the all-valid build needs fewer registers: one more resident CTA per SM
-  // where the general build is held to five
-  constexpr int MINB_A = (TY == 32 && MINB == 5) ? 6 : MINB;
+  // both builds under the same register cap (2048^2 step, all-valid build
+  // at 4 / 5 / 6 / 7 CTAs per SM: 130.6 / 121.3 / 129.6 / 139.5 us with
+  // steps back to back; 5 and 6 are level, 128.8 / 129.3 us, with L2 flushed
+  // between steps)
+  constexpr int MINB_A = MINB;
   auto *kg = rows_step_kernel<T, TY, FAST, MINB, SOURCES, 0>;
   auto *ka = rows_step_kernel<T, TY, FAST, MINB_A, SOURCES, 1>;
   static std::once_flag once;
