@@ -379,6 +379,8 @@ def run_ours(args) -> None:
 
 
 def strip_config(args, world: int) -> dict:
+    if not args.strips:
+        return {}
     if world > 1:
         halo = ("halo rows written by the step kernel through CUDA IPC peer mappings"
                 if args.peer else "NCCL halo exchange (2 rows of h, qx, qy each way)")
