@@ -153,11 +153,14 @@ int hb_fused_finish(const struct hb_fused_batch *batch, const double *ext, void 
  *  - prepare != 0 (re)initialises that scratch for this batch (as
  *    hb_fused_prepare does for a workspace), then runs nsteps steps; pass it
  *    on the first call and whenever the batch or its control blocks change.
- *  - Limits: hb_fused_workspace_size(b) <= 4 MiB (about 120,000 tiles, e.g.
- *    120 M cells with 32 x 32 tiles) and at most 256 instances; larger
- *    batches get HB_ERR_LIMIT with a message.
- *  - The first call on a device looks up the array's device address; make
- *    that first call before any stream capture.
+ *  - Limits: hb_fused_workspace_size(b) <= 4 MiB (about 110,000 tiles, e.g.
+ *    110 M cells with 32 x 32 tiles; about 100,000 with 256 instances) and at
+ *    most 256 instances; larger batches get HB_ERR_LIMIT with a message.
+ *  - The first call on a device looks up the array's device address, and the
+ *    first call with prepare != 0 on a device creates the library's side
+ *    stream and two events for that device (kept until exit; no device
+ *    memory is allocated for them by this library); make that first call
+ *    before any stream capture.
  *  - Every call on a device shares the one array and leaves its contents
  *    behind: calls that overlap on the GPU (other streams, other threads)
  *    race with each other. */
