@@ -45,6 +45,23 @@ extern "C" int refgpu_flux2(int M, int N, int dw, int dh, int ww, int wh, int qw
 }
 """,
     ),
+    # the 1st-order flux kernel has the 2nd-order one's name: renamed in its
+    # translation unit (PREFIX below) so that the two launch stubs stay apart
+    "fluxCal_jh_modified_surface_Kernel.cu": (
+        "void fluxCalculation_cuda(",
+        r"""
+extern "C" int refgpu_flux1(int M, int N, int dw, int dh, int ww, int wh, int qw, int qh,
+    int32_t *wet, double *h, double *wl, double *z, double *qx, double *qy,
+    int32_t *index, double *normal, double *gd, double *gw, double *gq,
+    double *dx, double *t, double *dt, double *hf, double *qxf, double *qyf, void *st) {
+  if (M == 0) return 0;
+  fluxCalculation_kernel<double><<<(M + 512 - 1) / 512, 512, 0, (cudaStream_t)st>>>(
+      M, N, dw, dh, ww, wh, qw, qh, wet, h, wl, z, qx, qy, index, normal, gd, gw, gq,
+      dx, t, dt, hf, qxf, qyf);
+  return (int)cudaGetLastError();
+}
+""",
+    ),
     "friction_implicit_andUpdate_jh_Kernel.cu": (
         "void frictionCalculation_cuda(",
         r"""
@@ -97,6 +114,11 @@ extern "C" int refgpu_flux_mask(int N, bool *out, double *h, int32_t *index, dou
     ),
 }
 
+PREFIX = {
+    "fluxCal_jh_modified_surface_Kernel.cu":
+        "#define fluxCalculation_kernel refgpu_first_order_fluxCalculation_kernel\n",
+}
+
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-w"]
 
@@ -126,7 +148,8 @@ def build(ref_root: str = DEFAULT_REF, verbose: bool = False, ptxas: bool = Fals
     objs = []
     cc = nvcc()
     for fname, (marker, launcher) in _LAUNCH.items():
-        text = '#include "ref_cuda_shim.h"\n' + _kernel_text(os.path.join(kdir, fname), marker)
+        text = ('#include "ref_cuda_shim.h"\n' + PREFIX.get(fname, "") +
+                _kernel_text(os.path.join(kdir, fname), marker))
         text += "\n" + launcher
         obj = os.path.join(OUT_DIR, os.path.splitext(fname)[0] + ".o")
         cmd = [cc, *NVCC_FLAGS, "-I", HERE, "-x", "cu", "-", "-c", "-o", obj]

@@ -34,11 +34,12 @@ class RefGpuOps:
             raise FileNotFoundError(f"{LIB} is not built (python baseline/build_ref_cuda.py)")
         L = ctypes.CDLL(LIB)
         L.refgpu_flux2.argtypes = [_I] * 8 + [_P] * 17 + [_P]
+        L.refgpu_flux1.argtypes = [_I] * 8 + [_P] * 17 + [_P]
         L.refgpu_friction_update.argtypes = [_I] + [_P] * 13 + [_P]
         L.refgpu_timestep.argtypes = [_I] + [_P] * 10 + [_P]
         L.refgpu_rain_station.argtypes = [_I] + [_P] * 4 + [_P]
         L.refgpu_flux_mask.argtypes = [_I] + [_P] * 4 + [_P]
-        for f in ("refgpu_flux2", "refgpu_friction_update", "refgpu_timestep",
+        for f in ("refgpu_flux2", "refgpu_flux1", "refgpu_friction_update", "refgpu_timestep",
                   "refgpu_rain_station", "refgpu_flux_mask"):
             getattr(L, f).restype = _I
         self._L = L
@@ -63,18 +64,24 @@ class RefGpuOps:
         self._ok(self._L.refgpu_flux_mask(h.numel(), *self._p(fluxMask, h, index, t),
                                           self._stream()), "fluxMask")
 
-    def flux_2nd_order(self, wetMask, h_flux, qx_flux, qy_flux, h, wl, z, qx, qy, index,
-                       normal, given_depth, given_wl, given_q, dx, t, dt):
+    def _flux(self, fn, wetMask, h_flux, qx_flux, qy_flux, h, wl, z, qx, qy, index, normal,
+              given_depth, given_wl, given_q, dx, t, dt):
         dh, dw = given_depth.shape
         wh, ww = given_wl.shape
         qh, qw = given_q.shape
-        self._ok(self._L.refgpu_flux2(
+        self._ok(fn(
             wetMask.numel(), h.numel(), dw, dh, ww, wh, qw, qh,
             *self._p(wetMask, h, wl, z, qx, qy, index, normal, given_depth, given_wl,
                      given_q, dx, t, dt, h_flux, qx_flux, qy_flux), self._stream()), "addFlux")
 
+    def flux_2nd_order(self, *args):
+        """HC/flucCal_2ndOrder_jh_improved_Kernel.cu (MUSCL + hydrostatic + HLLC)."""
+        self._flux(self._L.refgpu_flux2, *args)
+
     def flux_1st_order(self, *args):
-        raise NotImplementedError("only the 2nd-order reference flux kernel is bound")
+        """HC/fluxCal_jh_modified_surface_Kernel.cu (bed-only minmod + HLLC), the
+        scheme of the coupled server (CHANS-HiPIMS_server.py: secondOrder False)."""
+        self._flux(self._L.refgpu_flux1, *args)
 
     def friction_update(self, wetMask, h_update, qx_update, qy_update, z_update, landuse, h,
                         wl, qx, qy, z, manning, dt):

@@ -5,8 +5,9 @@
 Workload (the configuration the headline metric is quoted on): a 2048 x 2048
 urban catchment, 2 m cells, seeded Gaussian-random-field DEM (k^-3, 0-50 m)
 with 8 % of cells raised 10 m as buildings, 30 % road cells (n = 0.035, else
-0.08), open boundary ring, dry start, uniform rain 50 mm/h.  A step is one
-fused launch advancing every valid cell (4,194,304) by one time step.
+0.08), open boundary ring, dry start, uniform rain 50 mm/h.  A step advances
+every valid cell (4,194,304) by one time step: the general-tile and the
+all-valid-tile builds of the fused step kernel, launched at once.
 
 Timing: 8 untimed spin-up steps (the dry start becomes wet everywhere), W
 untimed warm-up steps, then K timed steps.  Each timed step is bracketed by
@@ -347,6 +348,8 @@ def run_ours(args) -> None:
         }
         if args.accuracy and world == 1 and not args.strips:
             line["accuracy"] = accuracy_vs_fp64(d, dev)
+        if args.first_order and world == 1:
+            line["first_order"] = first_order_rates(d, dev, args, flush, stream)
         if args.plain and world == 1:
             pl = plain_fp64_rate(d, dev, reference_kernels=True)
             if pl.get("value"):
@@ -392,7 +395,8 @@ def strip_config(args, world: int) -> dict:
                              f"by hb_fused_finish)"}
 
 
-def plain_fp64_rate(d: dict, dev, steps: int = 5, reference_kernels: bool = True) -> dict:
+def plain_fp64_rate(d: dict, dev, steps: int = 5, reference_kernels: bool = True,
+                    order: int = 2) -> dict:
     """The plain FP64 GPU path: the reference solver loop (Godunov object API,
     compacted cells, gather-based per-cell fluxes, host syncs per step) on the
     same catchment, wall-clock per step; with reference_kernels the ops are the
@@ -410,7 +414,7 @@ def plain_fp64_rate(d: dict, dev, steps: int = 5, reference_kernels: bool = True
         path = ("Godunov loop on the reference's own kernels built for sm_100a "
                 "(flux, fluxMask, friction-update, timeControl, station rain), torch.min, "
                 "wall clock")
-    g = Godunov(dev, d["dx"], d["cfl"], 1.0e30, secondOrder=True,
+    g = Godunov(dev, d["dx"], d["cfl"], 1.0e30, secondOrder=order == 2,
                 firstTimeStep=d["first_dt"], tensorType=torch.float64, ops_impl=impl)
     g._export_enabled = False
     T = lambda a: torch.as_tensor(np.asarray(a, dtype=np.float64))
@@ -437,6 +441,41 @@ def plain_fp64_rate(d: dict, dev, steps: int = 5, reference_kernels: bool = True
     n = int(g._h_internal.numel())
     return {"value": n * steps / el / 1e9, "unit": METRIC, "steps": steps, "dtype": "f64",
             "path": path}
+
+
+def first_order_rates(d: dict, dev, args, flush: torch.Tensor, stream, steps: int = 500) -> dict:
+    """The reference's 1st-order scheme (secondOrder False, the coupled
+    server's choice) on the same catchment: the fused FP32 step timed like the
+    main leg (CUDA events per step, L2 flushed between steps), and the
+    reference's own 1st-order kernels on the B200 under the Godunov loop."""
+    from hipims_b200.fused import FusedSolver
+    from hipims_b200.scenarios import catchment_from
+
+    fs = FusedSolver(catchment_from(d), dtype=torch.float32, tile=(32, 32), device=dev,
+                     minb=args.minb, order=1)
+    n = sum(i.n_valid for i in fs.inst)
+    fs.step(SPINUP + args.warmup)
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    for a, b in ev:
+        flush.fill_(1)
+        a.record(stream)
+        fs.step(1)
+        b.record(stream)
+    torch.cuda.synchronize(dev)
+    fs.check()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / steps
+    value = n / (ms * 1e-3) / 1e9
+    out = {"value": value, "unit": METRIC, "steps": steps, "ms_per_step": ms, "dtype": "f32",
+           "path": "FusedSolver(order=1): the two builds of the 1st-order step kernel, "
+                   "CUDA events per step, L2 flushed between steps"}
+    del fs
+    pl = plain_fp64_rate(d, dev, reference_kernels=True, order=1)
+    out["fp64_plain_first_order"] = pl
+    if pl.get("value"):
+        out["fused_fp32_over_plain"] = value / pl["value"]
+    return out
 
 
 def ensemble_rate(dev, steps: int, count: int = 64, seed: int = 0) -> dict:
@@ -678,6 +717,7 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-accuracy", dest="accuracy", action="store_false")
     ap.add_argument("--no-plain", dest="plain", action="store_false")
+    ap.add_argument("--no-first-order", dest="first_order", action="store_false")
     ap.add_argument("--no-ensemble", dest="ensemble", action="store_false")
     ap.add_argument("--ensemble-steps", type=int, default=20)
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false")

@@ -1023,11 +1023,16 @@ __device__ __forceinline__ Cell<T> edge_of(const Cell<T> &c, const Slope<T> &s, 
 
 // Face between valid cells A (west/south) and B (east/north) from A's side,
 // from the cells and their MUSCL slopes along DIR (0: normal +x, 1: +y).
+// ORDER 2: MUSCL edge states and the 2nd-order hydrostatic step
+// (HC/flucCal_2ndOrder_jh_improved_Kernel.cu:43-107, 410-485); ORDER 1:
+// piecewise-constant states, only the bed gets half its minmod slope, on a
+// side whose neighbour across the face is wet, and the 1st-order hydrostatic
+// step (HC/fluxCal_jh_modified_surface_Kernel.cu:96-139, 577-610).
 // FAST (FP32) evaluates the face with bed elevations measured from A's bed:
 // every operation of the scheme is invariant under a common shift of z, and
 // in that frame eta = h + z is rounded at the scale of the local relief
 // instead of the absolute elevation.
-template <typename T, bool FAST, int DIR>
+template <typename T, bool FAST, int DIR, int ORDER = 2>
 __device__ __forceinline__ FaceOut<T> face_edges(Cell<T> A, Cell<T> B, const Slope<T> &sA,
                                                  const Slope<T> &sB) {
   const T hs = T(kHSmall), g = T(kG);
@@ -1040,10 +1045,26 @@ __device__ __forceinline__ FaceOut<T> face_edges(Cell<T> A, Cell<T> B, const Slo
     A.wl = A.h;
     B.wl = B.z + B.h;
   }
-  Cell<T> eL = edge_of(A, sA, T(1));
-  Cell<T> eR = edge_of(B, sB, T(-1));
+  Cell<T> eL, eR;
+  if constexpr (ORDER == 1) {
+    eL = A;
+    eR = B;
+    if (B.h > hs) eL.z = A.z + T(0.5) * sA.z;
+    if (A.h > hs) eR.z = B.z + T(0.5) * (-sB.z);
+  } else {
+    eL = edge_of(A, sA, T(1));
+    eR = edge_of(B, sB, T(-1));
+  }
   T ux_l, uy_l, ux_r, uy_r;
-  if constexpr (FAST) {
+  if constexpr (FAST && ORDER == 1) {
+    // 1st order: the edge states are the cells themselves, so a row's two
+    // faces share these products; rounded on their own (no contraction into
+    // a later add), they come out the same in every build of the kernel
+    const T il = eL.h < hs ? T(0) : T(1) / eL.h;
+    const T ir = eR.h < hs ? T(0) : T(1) / eR.h;
+    ux_l = __fmul_rn(eL.qx, il); uy_l = __fmul_rn(eL.qy, il);
+    ux_r = __fmul_rn(eR.qx, ir); uy_r = __fmul_rn(eR.qy, ir);
+  } else if constexpr (FAST) {
     const T il = eL.h < hs ? T(0) : T(1) / eL.h;
     const T ir = eR.h < hs ? T(0) : T(1) / eR.h;
     ux_l = eL.qx * il; uy_l = eL.qy * il;
@@ -1054,7 +1075,10 @@ __device__ __forceinline__ FaceOut<T> face_edges(Cell<T> A, Cell<T> B, const Slo
     ux_r = eR.h < hs ? T(0) : eR.qx / eR.h;
     uy_r = eR.h < hs ? T(0) : eR.qy / eR.h;
   }
-  hydro2(A.wl, B.wl, eL, eR);
+  if constexpr (ORDER == 1)
+    hydro1(A.h, A.z, B.h, B.z, eL, eR);
+  else
+    hydro2(A.wl, B.wl, eL, eR);
   T Fh, Fn, Ft;
   if (DIR == 0) {
     if (hllc<T, FAST>(eL.h, eR.h, ux_l, ux_r, uy_l, uy_r, Fh, Fn, Ft)) {
@@ -1072,7 +1096,7 @@ __device__ __forceinline__ FaceOut<T> face_edges(Cell<T> A, Cell<T> B, const Slo
 
 // Boundary face of valid cell C with outward normal (n0, n1): ghost from
 // C's class.  Flux from C's side and C's bed-slope term.
-template <typename T, bool FAST>
+template <typename T, bool FAST, int ORDER = 2>
 __device__ __noinline__ void ghost_face(const Cell<T> C, int cls, int type, const double *bcv,
                                         T n0, T n1, T datum, T *out) {
   const T hs = T(kHSmall), g = T(kG);
@@ -1087,7 +1111,8 @@ __device__ __noinline__ void ghost_face(const Cell<T> C, int cls, int type, cons
     Cl.z = T(0);
     Cl.wl = Cl.h;
   }
-  if (!ghost(type, false, Cl, n0, n1, hb, wlbl, qxb, qyb, G)) return;
+  // FALL (type 9) is a ghost of the 1st-order scheme only
+  if (!ghost(type, ORDER == 1, Cl, n0, n1, hb, wlbl, qxb, qyb, G)) return;
   (void)cls;
   if (Cl.h < hs && G.h < hs) return;
   Cell<T> eL = Cl, eR = G;
@@ -1103,7 +1128,10 @@ __device__ __noinline__ void ghost_face(const Cell<T> C, int cls, int type, cons
     ux_r = eR.h < hs ? T(0) : eR.qx / eR.h;
     uy_r = eR.h < hs ? T(0) : eR.qy / eR.h;
   }
-  hydro2(Cl.wl, G.wl, eL, eR);
+  if constexpr (ORDER == 1)
+    hydro1(Cl.h, Cl.z, G.h, G.z, eL, eR);
+  else
+    hydro2(Cl.wl, G.wl, eL, eR);
   const T u_L = ux_l * n0 + uy_l * n1, u_R = ux_r * n0 + uy_r * n1;
   const T v_L = -ux_l * n1 + uy_l * n0, v_R = -ux_r * n1 + uy_r * n0;
   T Fh, Fn, Ft;
@@ -1137,23 +1165,23 @@ struct RowsView {
 // Face between A (minus side) and B (plus side) along DIR, any validity.
 // sA / sB: MUSCL slopes of A and B along DIR (used only when both are valid).
 // ALLV: both cells are known to be valid (no ghost face can occur).
-template <typename T, bool FAST, int DIR, int TY, bool ALLV = false>
+template <typename T, bool FAST, int DIR, int TY, bool ALLV = false, int ORDER = 2>
 __device__ __forceinline__ FaceOut<T> face_any(const RowsSmem<T, TY> &s, const Cell<T> &A,
                                                uint8_t ca, const Cell<T> &B, uint8_t cb,
                                                const Slope<T> &sA, const Slope<T> &sB, T datum) {
-  if constexpr (ALLV) return face_edges<T, FAST, DIR>(A, B, sA, sB);
+  if constexpr (ALLV) return face_edges<T, FAST, DIR, ORDER>(A, B, sA, sB);
   const bool va = is_valid(ca), vb = is_valid(cb);
-  if (va && vb) return face_edges<T, FAST, DIR>(A, B, sA, sB);
+  if (va && vb) return face_edges<T, FAST, DIR, ORDER>(A, B, sA, sB);
   FaceOut<T> o{T(0), T(0), T(0), T(0), T(0)};
   const T n0 = DIR == 0 ? T(1) : T(0), n1 = DIR == 0 ? T(0) : T(1);
   T out[4];
   if (va) {
     const int cls = ca >> 4;
-    ghost_face<T, FAST>(A, cls, s.bctype[cls], s.bc[cls], n0, n1, datum, out);
+    ghost_face<T, FAST, ORDER>(A, cls, s.bctype[cls], s.bc[cls], n0, n1, datum, out);
     o.fh = out[0]; o.fx = out[1]; o.fy = out[2]; o.sa = out[3];
   } else if (vb) {
     const int cls = cb >> 4;
-    ghost_face<T, FAST>(B, cls, s.bctype[cls], s.bc[cls], -n0, -n1, datum, out);
+    ghost_face<T, FAST, ORDER>(B, cls, s.bctype[cls], s.bc[cls], -n0, -n1, datum, out);
     o.fh = -out[0]; o.fx = -out[1]; o.fy = -out[2]; o.sb = out[3];
   }
   return o;
@@ -1167,7 +1195,7 @@ __device__ __forceinline__ FaceOut<T> face_any(const RowsSmem<T, TY> &s, const C
 // tiles registers, spills and about 9 % of their time when they share one).
 // order[0, counts[0]) are the general tiles, order[counts[0], counts[0] +
 // counts[1]) the all-valid ones.
-template <typename T, int TY, bool FAST, int MINB, bool SOURCES, int PATH>
+template <typename T, int TY, bool FAST, int MINB, bool SOURCES, int PATH, int ORDER>
 __global__ void __launch_bounds__(kRowsNT, MINB)
 rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restrict__ tile_inst,
                  const int32_t *__restrict__ order, const int32_t *__restrict__ counts,
@@ -1283,7 +1311,8 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
         const uint8_t ca = V.code(i, 31), cb = V.code(i, 32);
         const Slope<T> sa = slope_of(a, V.cell(i, 30), is_valid(V.code(i, 30)), b, is_valid(cb));
         const Slope<T> sb = slope_of(b, a, is_valid(ca), V.cell(i, 33), is_valid(V.code(i, 33)));
-        const FaceOut<T> f = face_any<T, FAST, 0, TY, kAllValid>(s, a, ca, b, cb, sa, sb, datum_tile);
+        const FaceOut<T> f =
+            face_any<T, FAST, 0, TY, kAllValid, ORDER>(s, a, ca, b, cb, sa, sb, datum_tile);
         s.xe[i][0] = f.fh;
         s.xe[i][1] = f.fx;
         s.xe[i][2] = f.fy;
@@ -1332,7 +1361,7 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
         syC = slope_of(cC, cS, valid(kS), cN, valid(kN));
         syS = slope_of(cS, cSS, valid(kSS), cC, valid(kC));
         // face between rows r0-1 (north) and r0 (south), from the south side
-        nf = face_any<T, FAST, 1, TY, ALLV>(s, cC, kC, cN, kN, syC, syN, datum_tile);
+        nf = face_any<T, FAST, 1, TY, ALLV, ORDER>(s, cC, kC, cN, kN, syC, syN, datum_tile);
       }
       __syncthreads();  // tile-edge faces and slopes ready
       T *hout = (T *)in.h[1 - cur];
@@ -1368,7 +1397,7 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
           sxW.qy = s.sxw[i][3];
         }
         // west face (this cell is B) -> the west neighbour's east face
-        const FaceOut<T> wf = face_any<T, FAST, 0, TY, ALLV>(s, cW, kW, cC, kC, sxW, sxC, datum_tile);
+        const FaceOut<T> wf = face_any<T, FAST, 0, TY, ALLV, ORDER>(s, cW, kW, cC, kC, sxW, sxC, datum_tile);
         T ef_h = __shfl_down_sync(0xffffffffu, wf.fh, 1);
         T ef_x = __shfl_down_sync(0xffffffffu, wf.fx, 1);
         T ef_y = __shfl_down_sync(0xffffffffu, wf.fy, 1);
@@ -1380,7 +1409,7 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
           ef_a = s.xe[i][3];
         }
         // south face (this cell is B, the row below is A)
-        const FaceOut<T> sf = face_any<T, FAST, 1, TY, ALLV>(s, cS, kS, cC, kC, syS, syC, datum_tile);
+        const FaceOut<T> sf = face_any<T, FAST, 1, TY, ALLV, ORDER>(s, cS, kS, cC, kC, syS, syC, datum_tile);
         const int ry = y0 + i;
         if (vC) {
           const T hc = cC.h;
@@ -1809,7 +1838,8 @@ int side_setup() {
   return HB_OK;
 }
 
-template <typename T, int TY, bool FAST = (sizeof(T) == 4), int MINB = 1, bool SOURCES = false>
+template <typename T, int TY, bool FAST = (sizeof(T) == 4), int MINB = 1, bool SOURCES = false,
+          int ORDER = 2>
 int launch_rows_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   using S = RowsSmem<T, TY>;
   // both builds under the same register cap (2048^2 step, all-valid build
@@ -1817,8 +1847,8 @@ int launch_rows_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   // steps back to back; 5 and 6 are level, 128.8 / 129.3 us, with L2 flushed
   // between steps)
   constexpr int MINB_A = MINB;
-  auto *kg = rows_step_kernel<T, TY, FAST, MINB, SOURCES, 0>;
-  auto *ka = rows_step_kernel<T, TY, FAST, MINB_A, SOURCES, 1>;
+  auto *kg = rows_step_kernel<T, TY, FAST, MINB, SOURCES, 0, ORDER>;
+  auto *ka = rows_step_kernel<T, TY, FAST, MINB_A, SOURCES, 1, ORDER>;
   static std::once_flag once;
   static cudaError_t attr_err = cudaSuccess;
   std::call_once(once, [&] {
@@ -1872,10 +1902,11 @@ int launch_rows_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
 
 // The build with the infiltration / station-rain branches when the batch
 // says its instances use them (HB_FLAG_SOURCES).
-template <typename T, int TY, bool FAST = (sizeof(T) == 4), int MINB = 1>
+template <typename T, int TY, bool FAST = (sizeof(T) == 4), int MINB = 1, int ORDER = 2>
 int launch_rows(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
-  if (b->flags & HB_FLAG_SOURCES) return launch_rows_impl<T, TY, FAST, MINB, true>(b, nsteps, st);
-  return launch_rows_impl<T, TY, FAST, MINB, false>(b, nsteps, st);
+  if (b->flags & HB_FLAG_SOURCES)
+    return launch_rows_impl<T, TY, FAST, MINB, true, ORDER>(b, nsteps, st);
+  return launch_rows_impl<T, TY, FAST, MINB, false, ORDER>(b, nsteps, st);
 }
 
 bool uses_rows_kernel(const hb_fused_batch *b) { return !(b->flags & HB_FLAG_TILE_TASKS); }
@@ -2081,11 +2112,26 @@ extern "C" int hb_fused_step(const hb_fused_batch *b, int nsteps, void *stream) 
   if (!b || !b->instances || !b->tile_instance || !b->workspace || b->n_tiles <= 0)
     return set_error(HB_ERR_ARG, "hb_fused_step: bad batch record");
   if (nsteps < 0) return set_error(HB_ERR_ARG, "hb_fused_step: negative nsteps");
-  if (b->order != 2) return set_error(HB_ERR_ARG, "hb_fused_step: only order 2 is fused");
+  if (b->order != 1 && b->order != 2)
+    return set_error(HB_ERR_ARG, "hb_fused_step: order %d (1 or 2)", b->order);
+  if (b->order == 1 && !uses_rows_kernel(b))
+    return set_error(HB_ERR_ARG, "hb_fused_step: the tile-task kernel is 2nd order only");
   if (nsteps == 0) return HB_OK;
   auto st = as_stream(stream);
   const int ty = b->tile_y, tx = b->tile_x;
   const bool exact = (b->flags & HB_FLAG_EXACT_FP32) != 0;
+  if (uses_rows_kernel(b) && b->order == 1) {
+    // the 1st-order scheme (the coupled server's): FP32 32 x 32 tiles, FP64
+    if (tx == kTW && ty == 32 && b->dtype == HB_F32 && !exact) {
+      const int minb = (b->flags >> HB_FLAG_MINB_SHIFT) & 0xF;
+      if (minb == 0) return launch_rows<float, 32, true, 1, 1>(b, nsteps, st);
+      if (minb == 5) return launch_rows<float, 32, true, 5, 1>(b, nsteps, st);
+    }
+    if (tx == kTW && ty == 32 && b->dtype == HB_F64)
+      return launch_rows<double, 32, false, 1, 1>(b, nsteps, st);
+    return set_error(HB_ERR_ARG, "hb_fused_step: order 1 is built for 32 x 32 tiles, FP32 (fast, "
+                                 "minb 0 or 5) and FP64");
+  }
   if (uses_rows_kernel(b)) {
     if (tx != kTW) return set_error(HB_ERR_ARG, "hb_fused_step: rows kernel tiles are 32 wide");
     if (b->dtype == HB_F32 && exact) {

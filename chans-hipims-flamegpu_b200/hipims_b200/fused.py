@@ -202,19 +202,30 @@ class _Instance:
 
 
 class FusedSolver:
-    """Advance one or more catchments with the fused dense-tile kernel."""
+    """Advance one or more catchments with the fused dense-tile kernel.
+
+    order 2 (default): the reference's 2nd-order scheme (MUSCL, `secondOrder`
+    True); order 1: its 1st-order scheme (`secondOrder` False, the coupled
+    server's choice, CHANS-HiPIMS_server.py), rows kernel with 32 x 32 tiles."""
 
     def __init__(self, catchments: Catchment | Sequence[Catchment], dtype=torch.float32,
                  tile: tuple[int, int] | None = None, device="cuda", grid_blocks: int = 0,
-                 exact_fp32: bool = False, kernel: str = "rows", minb: int = 0):
+                 exact_fp32: bool = False, kernel: str = "rows", minb: int = 0,
+                 order: int = 2):
         if isinstance(catchments, Catchment):
             catchments = [catchments]
         if dtype not in (torch.float32, torch.float64):
             raise ValueError("dtype must be float32 or float64")
+        if order not in (1, 2):
+            raise ValueError("order must be 1 or 2")
+        if order == 1 and kernel != "rows":
+            raise ValueError("the 1st-order scheme runs in the rows kernel")
         self.device = torch.device(device)
         self.dtype = dtype
-        if tile is None:  # rows kernel: 32 wide; 64 high in FP32, 32 high in FP64
-            tile = (64, 32) if dtype == torch.float32 and kernel == "rows" else (32, 32)
+        self.order = order
+        if tile is None:  # rows kernel: 32 wide; 64 high in FP32 order 2, else 32 high
+            tile = (64, 32) if dtype == torch.float32 and kernel == "rows" and order == 2 \
+                else (32, 32)
         self.tile = tuple(tile)
         self.inst = [_Instance(c, dtype, self.device, self.tile) for c in catchments]
         n = len(self.inst)
@@ -295,7 +306,7 @@ class FusedSolver:
         b.n_tiles = self.n_tiles
         b.tile_y, b.tile_x = self.tile
         b.grid_blocks = grid_blocks
-        b.order = 2
+        b.order = order
         sources = any(i.cum is not None or i.rain_station is not None for i in self.inst)
         b.flags = ((1 if exact_fp32 else 0) | (2 if kernel == "tasks" else 0) |
                    (4 if sources else 0) | (minb << 8))
