@@ -47,7 +47,9 @@ class FusedBackend:
 
     agent_rows / agent_cols: raster positions of the agent cells, in the
     order the reference reports them (ascending compacted id = row-major order
-    of the valid cells, `CHANS-HiPIMS_server.py:140-153`).
+    of the valid cells, `CHANS-HiPIMS_server.py:140-153`).  The reference
+    server runs the 1st-order scheme (its `'secondOrder': False`): build the
+    solver with `FusedSolver(..., order=1)` to match it.
     """
 
     def __init__(self, solver: FusedSolver, agent_rows, agent_cols, instance: int = 0,
