@@ -585,10 +585,12 @@ def adjoint_cost(dev, n: int = 1024, steps: int = 2000, K: int = 100, every: int
 def coupled_rate(dev, n: int = 8192, sim_seconds: float = 120.0, period: float = 60.0,
                  agents: int = 100_000, tile=(32, 32), minb: int = 5) -> dict:
     """Config 5: an n x n catchment (1 m cells, rain 100 mm/h, Q_GIVEN inflow
-    hydrograph on one edge) advanced by the fused FP32 step from a dry start;
-    every `period` simulated seconds the agent cells' depth and velocities are
-    gathered on the device, copied to the host and serialised with msgpack, as
-    the RPC server's request_data answer.  Wall clock over the whole run."""
+    hydrograph on one edge) advanced by the fused FP32 step from a dry start,
+    in the 1st-order scheme the reference's coupled server runs
+    (CHANS-HiPIMS_server.py: secondOrder False); every `period` simulated
+    seconds the agent cells' depth and velocities are gathered on the device,
+    copied to the host and serialised with msgpack, as the RPC server's
+    request_data answer.  Wall clock over the whole run."""
     import msgpack
 
     from hipims_b200 import scenarios as S
@@ -598,7 +600,7 @@ def coupled_rate(dev, n: int = 8192, sim_seconds: float = 120.0, period: float =
 
     d = S.coupled_case(n, agents=agents)
     fs = FusedSolver(catchment_from(d, t_end=sim_seconds), dtype=torch.float32,
-                     tile=tuple(tile), device=dev, minb=minb)
+                     tile=tuple(tile), device=dev, minb=minb, order=1)
     be = FusedBackend(fs, d["agent_rows"], d["agent_cols"], velocities=True)
     cells = fs.inst[0].n_valid
     del d
@@ -627,6 +629,7 @@ def coupled_rate(dev, n: int = 8192, sim_seconds: float = 120.0, period: float =
             "coupling_overhead": t_couple / total, "payload_bytes": nbytes,
             "hbm_achieved_gbs": achieved, "hbm_frac": achieved / peak,
             "peak_source": peak_kind,
+            "scheme": "1st order (the coupled server's)",
             "path": "FusedSolver.run_until (chunks of 128 launches, control-block read per "
                     "chunk) + hb_gather of h, u, v + D2H + msgpack, wall clock"}
 
