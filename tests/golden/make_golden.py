@@ -57,8 +57,54 @@ def mixed_bc_case(seed: int, order: int) -> dict:
                 export_step=0.75, steps=60, types=np.array(types))
 
 
+def edge_case(name: str) -> dict:
+    """Small and degenerate catchments, all boundaries RIGID (type 3) unless
+    noted, bumpy bed (0-5 cm), 40 steps, export clip every 0.25 s:
+      tiny3x5    3 x 5 cells (smaller than a tile), one wet cell in the middle
+      row1x40    a single row, dam break along it
+      col40x1    a single column, dam break along it (the RIGID ghost keeps
+                 the normal momentum on north/south faces, so water crosses
+                 the column's end walls, as in the reference)
+      dry        20 x 30 OPEN ring, no water, no rain: dt grows tenfold per
+                 step to the export clip
+      late_rain  the dry case with rain from t = 0.06 s"""
+    ny, nx, bc, wet, rain = {
+        "tiny3x5": (3, 5, 30, "column", None),
+        "row1x40": (1, 40, 30, "dam", None),
+        "col40x1": (40, 1, 30, "dam", None),
+        "dry": (20, 30, 50, "none", None),
+        "late_rain": (20, 30, 50, "none",
+                      np.array([[0.0, 0.0], [0.05, 0.0], [0.06, 2e-3], [100.0, 2e-3]])),
+    }[name]
+    rng = np.random.default_rng(len(name))
+    nodata = np.ones((ny + 2, nx + 2), dtype=bool)
+    nodata[1:-1, 1:-1] = False
+    mask = boundary_codes(nodata, default_bc=bc)
+    z = rng.uniform(0.0, 0.05, mask.shape)
+    h = np.zeros(mask.shape)
+    if wet == "dam":
+        r, c = np.meshgrid(np.arange(ny + 2), np.arange(nx + 2), indexing="ij")
+        h[:] = np.where((c <= (nx + 1) // 2) & (r <= (ny + 1) // 2 + (ny == 1)), 0.6, 0.05)
+    elif wet == "column":
+        h[(ny + 2) // 2, (nx + 2) // 2] = 1.0
+    h[nodata] = 0.0
+    zeros = np.zeros(mask.shape)
+    d = dict(mask=mask, z=z, h=h, qx=zeros.copy(), qy=zeros.copy(), wl=z + h,
+             landuse=np.zeros(mask.shape, dtype=np.uint8), manning=[0.03], dx=1.0, cfl=0.5,
+             first_dt=1.0e-4, export_step=0.25, steps=40)
+    if rain is not None:
+        d["rain"] = rain
+    return d
+
+
+EDGE_CASES = ("tiny3x5", "row1x40", "col40x1", "dry", "late_rain")
+
+
 def cases() -> dict:
     out = {}
+    for name in EDGE_CASES:
+        for order in (1, 2):
+            out[f"edge_{name}_o{order}"] = (edge_case(name), order)
     d = S.dam_break(48)
     d.update(steps=120)
     out["dam_break48_o2"] = (d, 2)
