@@ -991,16 +991,20 @@ struct Slope {
 // minmod slope of cell c between its minus-side neighbour m and plus-side
 // neighbour p; a no-data neighbour is replaced by c itself, as the reference
 // does with a missing neighbour id (HC/flucCal_2ndOrder_jh_improved_Kernel.cu:416-428).
-template <typename T>
+// The 1st-order scheme uses only the bed's slope
+// (HC/fluxCal_jh_modified_surface_Kernel.cu:577-610); its other fields are 0.
+template <int ORDER = 2, typename T>
 __device__ __forceinline__ Slope<T> slope_of(const Cell<T> &c, const Cell<T> &m, bool vm,
                                              const Cell<T> &p, bool vp) {
   const Cell<T> &mm = vm ? m : c;
   const Cell<T> &pp = vp ? p : c;
-  Slope<T> s;
-  s.h = minmod(c.h - mm.h, pp.h - c.h);
+  Slope<T> s{T(0), T(0), T(0), T(0)};
   s.z = minmod(c.z - mm.z, pp.z - c.z);
-  s.qx = minmod(c.qx - mm.qx, pp.qx - c.qx);
-  s.qy = minmod(c.qy - mm.qy, pp.qy - c.qy);
+  if constexpr (ORDER == 2) {
+    s.h = minmod(c.h - mm.h, pp.h - c.h);
+    s.qx = minmod(c.qx - mm.qx, pp.qx - c.qx);
+    s.qy = minmod(c.qy - mm.qy, pp.qy - c.qy);
+  }
   return s;
 }
 
@@ -1309,8 +1313,8 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
       for (int i = lane; i < TY; i += 32) {
         const Cell<T> a = V.cell(i, 31), b = V.cell(i, 32);
         const uint8_t ca = V.code(i, 31), cb = V.code(i, 32);
-        const Slope<T> sa = slope_of(a, V.cell(i, 30), is_valid(V.code(i, 30)), b, is_valid(cb));
-        const Slope<T> sb = slope_of(b, a, is_valid(ca), V.cell(i, 33), is_valid(V.code(i, 33)));
+        const Slope<T> sa = slope_of<ORDER>(a, V.cell(i, 30), is_valid(V.code(i, 30)), b, is_valid(cb));
+        const Slope<T> sb = slope_of<ORDER>(b, a, is_valid(ca), V.cell(i, 33), is_valid(V.code(i, 33)));
         const FaceOut<T> f =
             face_any<T, FAST, 0, TY, kAllValid, ORDER>(s, a, ca, b, cb, sa, sb, datum_tile);
         s.xe[i][0] = f.fh;
@@ -1321,7 +1325,7 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
     } else if (w == 1) {
       for (int i = lane; i < TY; i += 32) {
         const Cell<T> cm2 = V.cell(i, -2), cm1 = V.cell(i, -1), c0 = V.cell(i, 0);
-        const Slope<T> sm1 = slope_of(cm1, cm2, is_valid(V.code(i, -2)), c0,
+        const Slope<T> sm1 = slope_of<ORDER>(cm1, cm2, is_valid(V.code(i, -2)), c0,
                                       is_valid(V.code(i, 0)));
         s.sxw[i][0] = sm1.h;
         s.sxw[i][1] = sm1.z;
@@ -1357,9 +1361,9 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
         const Cell<T> cSS = V.cell(r0 + 2, j);
         const uint8_t kSS = V.code(r0 + 2, j);
         // y-slopes: minus side = south (row + 1), plus side = north (row - 1)
-        const Slope<T> syN = slope_of(cN, cC, valid(kC), cNN, valid(kNN));
-        syC = slope_of(cC, cS, valid(kS), cN, valid(kN));
-        syS = slope_of(cS, cSS, valid(kSS), cC, valid(kC));
+        const Slope<T> syN = slope_of<ORDER>(cN, cC, valid(kC), cNN, valid(kNN));
+        syC = slope_of<ORDER>(cC, cS, valid(kS), cN, valid(kN));
+        syS = slope_of<ORDER>(cS, cSS, valid(kSS), cC, valid(kC));
         // face between rows r0-1 (north) and r0 (south), from the south side
         nf = face_any<T, FAST, 1, TY, ALLV, ORDER>(s, cC, kC, cN, kN, syC, syN, datum_tile);
       }
@@ -1384,17 +1388,21 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
         const Cell<T> cW = V.cell(i, j - 1), cE = V.cell(i, j + 1);
         const uint8_t kW = V.code(i, j - 1), kE = V.code(i, j + 1);
         const bool vW = valid(kW), vE = valid(kE), vC = valid(kC);
-        const Slope<T> sxC = slope_of(cC, cW, vW, cE, vE);
-        Slope<T> sxW;
-        sxW.h = __shfl_up_sync(0xffffffffu, sxC.h, 1);
+        const Slope<T> sxC = slope_of<ORDER>(cC, cW, vW, cE, vE);
+        Slope<T> sxW{T(0), T(0), T(0), T(0)};
         sxW.z = __shfl_up_sync(0xffffffffu, sxC.z, 1);
-        sxW.qx = __shfl_up_sync(0xffffffffu, sxC.qx, 1);
-        sxW.qy = __shfl_up_sync(0xffffffffu, sxC.qy, 1);
+        if constexpr (ORDER == 2) {
+          sxW.h = __shfl_up_sync(0xffffffffu, sxC.h, 1);
+          sxW.qx = __shfl_up_sync(0xffffffffu, sxC.qx, 1);
+          sxW.qy = __shfl_up_sync(0xffffffffu, sxC.qy, 1);
+        }
         if (lane == 0) {
-          sxW.h = s.sxw[i][0];
           sxW.z = s.sxw[i][1];
-          sxW.qx = s.sxw[i][2];
-          sxW.qy = s.sxw[i][3];
+          if constexpr (ORDER == 2) {
+            sxW.h = s.sxw[i][0];
+            sxW.qx = s.sxw[i][2];
+            sxW.qy = s.sxw[i][3];
+          }
         }
         // west face (this cell is B) -> the west neighbour's east face
         const FaceOut<T> wf = face_any<T, FAST, 0, TY, ALLV, ORDER>(s, cW, kW, cC, kC, sxW, sxC, datum_tile);
@@ -1586,7 +1594,7 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
           kS = V.code(i + 2, j);
           const Cell<T> cSS = V.cell(i + 3, j);
           const uint8_t kSS = V.code(i + 3, j);
-          syS = slope_of(cS, cSS, valid(kSS), cC, valid(kC));
+          syS = slope_of<ORDER>(cS, cSS, valid(kSS), cC, valid(kC));
         }
       }
 
