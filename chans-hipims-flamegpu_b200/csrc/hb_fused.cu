@@ -199,7 +199,8 @@ __device__ __forceinline__ double warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
-__device__ __forceinline__ double warp_max(double v) {
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
@@ -1283,19 +1284,32 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
       __syncthreads();  // ddatum visible
       const int by0 = (y0 / HB_DATUM_BLOCK) * HB_DATUM_BLOCK;
       const int bx0 = (x0 / HB_DATUM_BLOCK) * HB_DATUM_BLOCK;
-      // halo rows (2 above, 2 below) and halo columns (4 each side)
-      constexpr int NH = 4 * kSWF + TY * 8;
+      // the halo sides that lie in another datum block: the 2 rows above
+      // (tile at the block's top) or below (at its bottom), full width, and
+      // the 4 columns left or right (tile at the block's left or right
+      // edge) over the rows the row sides leave out; the tile itself lies
+      // inside one block
+      const int nT = y0 == by0 ? 2 * kSWF : 0;
+      const int nB = y0 + TY == by0 + HB_DATUM_BLOCK ? 2 * kSWF : 0;
+      const int rlo = nT ? 0 : -2, rn = (nB ? TY : TY + 2) - rlo;
+      const int nL = x0 == bx0 ? 4 * rn : 0;
+      const int nR = x0 + kTW == bx0 + HB_DATUM_BLOCK ? 4 * rn : 0;
+      const int NH = nT + nB + nL + nR;
       for (int k = tid; k < NH; k += kRowsNT) {
-        int i, j;
-        if (k < 4 * kSWF) {
-          const int r = k / kSWF;
-          i = r < 2 ? r - 2 : TY + (r - 2);
-          j = k % kSWF - 4;
+        int i, j, q = k;
+        if (q < nT) {
+          i = q / kSWF - 2;
+          j = q % kSWF - 4;
+        } else if ((q -= nT) < nB) {
+          i = TY + q / kSWF;
+          j = q % kSWF - 4;
+        } else if ((q -= nB) < nL) {
+          i = rlo + (q >> 2);
+          j = (q & 3) - 4;
         } else {
-          const int q = k - 4 * kSWF;
-          i = q / 8;
-          const int c = q % 8;
-          j = c < 4 ? c - 4 : kTW + (c - 4);
+          q -= nL;
+          i = rlo + (q >> 2);
+          j = kTW + (q & 3);
         }
         const int ry = y0 + i, rx = x0 + j;
         const int dyb = ry < by0 ? 0 : (ry >= by0 + HB_DATUM_BLOCK ? 2 : 1);
@@ -1603,8 +1617,10 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
 
     // --- tile partials and the instance's last-tile finalize
     double vol = warp_sum((double)vol_t);
-    outf = warp_sum(outf);
-    double smax = warp_max((double)smax_t);
+    // an all-valid tile has no boundary face, so no outflow to sum; the
+    // maximum is exact in T
+    if constexpr (!kAllValid) outf = warp_sum(outf);
+    const double smax = (double)warp_max(smax_t);
     any_dry = __any_sync(0xffffffffu, any_dry);
     if (lane == 0) {
       s.red_d[0][w] = vol;
