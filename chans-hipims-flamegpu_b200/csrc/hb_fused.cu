@@ -1253,8 +1253,10 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
       tma_load_2d(s.code, m + 8, x0, y0, &s.bar);
     }
     if (tid < HB_MAX_CLASSES) {
-      s.bctype[tid] = in.bc_type[tid];
-      for (int q = 0; q < 4; q++) s.bc[tid][q] = bct[ii].v[tid][q];
+      if constexpr (!kAllValid) {  // ghost faces only
+        s.bctype[tid] = in.bc_type[tid];
+        for (int q = 0; q < 4; q++) s.bc[tid][q] = bct[ii].v[tid][q];
+      }
     } else if (tid >= 64 && tid < 64 + HB_MAX_ZONES) {
       s.manning[tid - 64] = (T)in.manning[tid - 64];
     }
