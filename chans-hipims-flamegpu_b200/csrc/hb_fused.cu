@@ -36,6 +36,7 @@
 #include <vector>
 
 #include "hb_common.cuh"
+#include "hb_datum_halo.cuh"
 #include "hb_physics.cuh"
 #include "hipims_b200_fused.h"
 
@@ -1286,33 +1287,12 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
       __syncthreads();  // ddatum visible
       const int by0 = (y0 / HB_DATUM_BLOCK) * HB_DATUM_BLOCK;
       const int bx0 = (x0 / HB_DATUM_BLOCK) * HB_DATUM_BLOCK;
-      // the halo sides that lie in another datum block: the 2 rows above
-      // (tile at the block's top) or below (at its bottom), full width, and
-      // the 4 columns left or right (tile at the block's left or right
-      // edge) over the rows the row sides leave out; the tile itself lies
-      // inside one block
-      const int nT = y0 == by0 ? 2 * kSWF : 0;
-      const int nB = y0 + TY == by0 + HB_DATUM_BLOCK ? 2 * kSWF : 0;
-      const int rlo = nT ? 0 : -2, rn = (nB ? TY : TY + 2) - rlo;
-      const int nL = x0 == bx0 ? 4 * rn : 0;
-      const int nR = x0 + kTW == bx0 + HB_DATUM_BLOCK ? 4 * rn : 0;
-      const int NH = nT + nB + nL + nR;
+      // only the halo sides that lie in another datum block
+      const DatumHalo dh = datum_halo(y0, x0, by0, bx0, TY, kTW, kSWF, HB_DATUM_BLOCK);
+      const int NH = dh.count();
       for (int k = tid; k < NH; k += kRowsNT) {
-        int i, j, q = k;
-        if (q < nT) {
-          i = q / kSWF - 2;
-          j = q % kSWF - 4;
-        } else if ((q -= nT) < nB) {
-          i = TY + q / kSWF;
-          j = q % kSWF - 4;
-        } else if ((q -= nB) < nL) {
-          i = rlo + (q >> 2);
-          j = (q & 3) - 4;
-        } else {
-          q -= nL;
-          i = rlo + (q >> 2);
-          j = kTW + (q & 3);
-        }
+        int i, j;
+        datum_halo_cell(dh, k, TY, kTW, kSWF, i, j);
         const int ry = y0 + i, rx = x0 + j;
         const int dyb = ry < by0 ? 0 : (ry >= by0 + HB_DATUM_BLOCK ? 2 : 1);
         const int dxb = rx < bx0 ? 0 : (rx >= bx0 + HB_DATUM_BLOCK ? 2 : 1);
