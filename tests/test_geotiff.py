@@ -1,8 +1,6 @@
 """GeoTIFF output (the reference's exportRaster_tiff, HP/postProcessing.py:26-196,
 without rasterio): pixels and tags read back with Pillow, and the reference's
 naming and scatter of exported field files."""
-import os
-
 import numpy as np
 import pytest
 import torch

@@ -5,7 +5,6 @@ exact up to the HLLC solver's round-off asymmetry, so the tolerance is 1e-10 m.
 FP32 fused: compared with the FP64 oracle at identical simulated times (the
 oracle's dt sequence is replayed) with the north-star tolerance, max depth
 error <= 1e-4 m; the adaptive FP32 run is checked too."""
-import math
 import os
 
 import numpy as np

@@ -5,7 +5,7 @@ import pytest
 import torch
 
 from hipims_b200 import _lib, scenarios as S, topology as T
-from hipims_b200.fused import Catchment, _Instance
+from hipims_b200.fused import _Instance
 from oracle import oracle as O
 
 

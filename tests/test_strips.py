@@ -11,7 +11,6 @@ import pytest
 import torch
 import torch.multiprocessing as mp
 
-from hipims_b200 import _lib
 from hipims_b200.strips import HALO, exchange_halos, split_rows
 
 
