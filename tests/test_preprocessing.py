@@ -138,3 +138,26 @@ def test_imported_rasters_drive_the_oracle_like_the_raster_index_coding(tmp_path
     assert sa["t"] == sb["t"] and np.isfinite(sa["h"]).all()
     for f in ("h", "qx", "qy"):
         np.testing.assert_array_equal(sa[f], sb[f])
+
+
+def test_export_raster_tiff_on_the_dem_grid(tmp_path):
+    """exportRaster_tiff(DEM_path, outPutPath) as HP/postProcessing.py:26-196:
+    each exported field file goes to the DEM's valid cells, -9999 elsewhere,
+    with the DEM's georeferencing, under the reference's name."""
+    from hipims_b200.geotiff import read_geotiff
+    from hipims_b200.postprocessing import exportRaster_tiff
+
+    path, _, nodata = _dem(tmp_path)
+    out = tmp_path / "out"
+    out.mkdir()
+    n = int((~nodata).sum())
+    vec = torch.arange(n, dtype=torch.float64) * 0.01
+    torch.save(vec, str(out / "h_tensor([3600.], device='cuda:0').pt"))
+    torch.save(-vec, str(out / "qx_tensor([3600.], device='cuda:0').pt"))
+    written = sorted(exportRaster_tiff(path, str(out)))
+    assert [p.rsplit("/", 1)[1] for p in written] == ["h_3600.tif", "qx_3600.tif"]
+    r, meta = read_geotiff(str(out / "h_3600.tif"))
+    assert r.dtype == np.float32 and meta["transform"] == T and meta["crs"] == "EPSG:27700"
+    assert meta["nodata"] == -9999.0
+    np.testing.assert_array_equal(r[~nodata], vec.numpy().astype(np.float32))
+    assert (r[nodata] == -9999.0).all()
