@@ -208,3 +208,101 @@ def test_oracle_matches_reference_build_on_random_shapes(order):
         assert sa["t"] == sb["t"], seed
         for k in FIELDS:
             np.testing.assert_array_equal(sa[k], sb[k], err_msg=f"seed {seed} {k}")
+
+
+def _radial_dam_break(n: int = 64) -> dict:
+    """A column of water (radius n/5, 1 m over 0.1 m) in the middle of an
+    n x n flat frictionless box with slip walls."""
+    from hipims_b200.topology import boundary_codes
+
+    nodata = np.ones((n + 2, n + 2), dtype=bool)
+    nodata[1:-1, 1:-1] = False
+    mask = boundary_codes(nodata, default_bc=40)
+    r, c = np.meshgrid(np.arange(n + 2) - (n + 1) / 2, np.arange(n + 2) - (n + 1) / 2,
+                       indexing="ij")
+    h = np.where(r ** 2 + c ** 2 < (n / 5) ** 2, 1.0, 0.1)
+    h[nodata] = 0.0
+    z = np.zeros_like(h)
+    return dict(mask=mask, z=z, h=h, qx=np.zeros_like(h), qy=np.zeros_like(h), wl=z + h,
+                manning=[0.0], dx=1.0, cfl=0.5, first_dt=1.0e-3)
+
+
+@pytest.mark.parametrize("order", [1, 2])
+@pytest.mark.parametrize("backend", ["oracle", "ref"])
+def test_physics_radial_dam_break_symmetry(order, backend):
+    """Mirror in x and in y and the swap of the axes leave a radial dam break
+    unchanged to round-off (the y axis of the rasters points south, so under
+    the swap qx(r, c) = -qy(c, r))."""
+    if backend == "ref" and not O.ref_available():
+        pytest.skip("oracle/_ref not built")
+    n = 64
+    s = O.Sim(_radial_dam_break(n), order=order, backend=backend)
+    s.run(60)
+    H, QX, QY = (a.reshape(n, n) for a in (s.h, s.qx, s.qy))
+    assert H.max() < 0.9  # the column has collapsed
+    tol = 1e-13
+    assert np.abs(H - H[:, ::-1]).max() < tol and np.abs(QX + QX[:, ::-1]).max() < tol
+    assert np.abs(H - H[::-1, :]).max() < tol and np.abs(QY + QY[::-1, :]).max() < tol
+    assert np.abs(H - H.T).max() < tol and np.abs(QX + QY.T).max() < tol
+
+
+def _stoker(x, t, hl, hr, x0):
+    """Stoker's solution of the frictionless wet/wet dam break: rarefaction,
+    constant middle state (h_m, u_m) and a shock into the still water."""
+    from scipy.optimize import brentq
+
+    g = 9.81
+    cl = np.sqrt(g * hl)
+
+    def momentum_jump(cm):
+        hm = cm * cm / g
+        um = 2.0 * (cl - cm)
+        s = hm * um / (hm - hr)
+        return s * hm * um - (hm * um * um + 0.5 * g * (hm * hm - hr * hr))
+
+    cm = brentq(momentum_jump, np.sqrt(g * hr) * (1 + 1e-9), cl * (1 - 1e-9))
+    hm, um = cm * cm / g, 2.0 * (cl - cm)
+    s = hm * um / (hm - hr)
+    xi = (x - x0) / t
+    h = np.where(xi < -cl, hl, np.where(xi < um - cm, ((2 * cl - xi) / 3) ** 2 / g,
+                                        np.where(xi < s, hm, hr)))
+    return h, hm, s
+
+
+def _dam_break_1d(n: int, order: int, t_end: float, hl: float = 1.0, hr: float = 0.1):
+    from hipims_b200.topology import boundary_codes
+
+    nodata = np.ones((3, n + 2), dtype=bool)
+    nodata[1, 1:-1] = False
+    mask = boundary_codes(nodata, default_bc=50)
+    x = np.arange(n + 2) - 0.5
+    h = np.where(x[None, :] < n / 2, hl, hr) * np.ones((3, 1))
+    h[nodata] = 0.0
+    z = np.zeros_like(h)
+    d = dict(mask=mask, z=z, h=h, qx=np.zeros_like(h), qy=np.zeros_like(h), wl=z + h,
+             manning=[0.0], dx=1.0, cfl=0.5, first_dt=1.0e-3)
+    sim = O.Sim(d, order=order, export_step=t_end)  # the export clip lands on t_end
+    sim.run(100000, t_end)
+    xc = np.arange(1, n + 1) - 0.5
+    return sim, xc, _stoker(xc, sim.t, hl, hr, n / 2)
+
+
+@pytest.mark.parametrize("order,l1", [(1, 0.004), (2, 0.0015)])
+def test_physics_stoker_dam_break(order, l1):
+    """The frictionless 1-D dam break (1 m over 0.1 m) against Stoker's
+    solution: mean depth error, shock position within a cell, qy = 0, and the
+    error shrinking with the grid."""
+    sim, xc, (exact, hm, s) = _dam_break_1d(400, order, 20.0)
+    assert sim.t == 20.0
+    err = np.abs(sim.h - exact)
+    assert err.mean() < l1, err.mean()
+    mid = 0.5 * (hm + 0.1)
+    j = np.where((sim.h[:-1] >= mid) & (sim.h[1:] < mid))[0][-1]
+    shock = xc[j] + (sim.h[j] - mid) / (sim.h[j] - sim.h[j + 1])
+    assert abs(shock - (200.0 + s * 20.0)) < 1.0
+    assert not np.any(sim.qy)
+    coarse = _dam_break_1d(200, order, 10.0)
+    fine = _dam_break_1d(800, order, 40.0)
+    e_coarse = np.abs(coarse[0].h - coarse[2][0]).mean()
+    e_fine = np.abs(fine[0].h - fine[2][0]).mean()
+    assert e_fine < 0.7 * e_coarse, (e_coarse, e_fine)
