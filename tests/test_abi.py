@@ -102,3 +102,20 @@ def test_dropin_ops_check_inputs_like_the_reference():
     i = torch.zeros(4, dtype=torch.int32)
     with pytest.raises(RuntimeError, match="h must be a CUDA tensor"):
         F.addFlux(i, x, x, x, x, x, x, x, x, i, x, x, x, x, x, x, x)
+
+
+def test_noalloc_limit_matches_the_documented_tile_counts():
+    """hb_fused_step_noalloc keeps its scratch in 4 MiB: the header's limits
+    (about 110,000 tiles, about 100,000 with 256 instances) hold for the
+    workspace size the library computes (pure host arithmetic)."""
+    L = _lib.lib()
+
+    def size(tiles, instances):
+        b = _lib.HbFusedBatch()
+        b.n_tiles, b.n_instances = tiles, instances
+        return L.hb_fused_workspace_size(ctypes.byref(b))
+
+    mib4 = 4 << 20
+    assert size(110_000, 1) <= mib4 < size(115_000, 1)
+    assert size(100_000, 256) <= mib4 < size(105_000, 256)
+    assert size(2, 1) < size(2, 2) < size(3, 2)  # grows with tiles and instances
