@@ -118,4 +118,5 @@ def test_noalloc_limit_matches_the_documented_tile_counts():
     mib4 = 4 << 20
     assert size(110_000, 1) <= mib4 < size(115_000, 1)
     assert size(100_000, 256) <= mib4 < size(105_000, 256)
-    assert size(2, 1) < size(2, 2) < size(3, 2)  # grows with tiles and instances
+    # grows with tiles and instances (regions are 256-byte aligned, so by steps)
+    assert size(1000, 1) < size(2000, 1) and size(1000, 1) < size(1000, 8)
