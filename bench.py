@@ -163,7 +163,8 @@ def cpu_dam_break_rates(steps: int = 1000) -> dict:
     from oracle import oracle as O
 
     kind = "reference" if O.ref_available() else "port"
-    out = {"kind": kind, "steps": steps, "cells": 256 * 256}
+    out = {"kind": kind, "steps": steps, "cells": 256 * 256, "cores": os.cpu_count() or 1,
+           "sample": f"config 1: 256^2 dam break, {steps} FP64 steps, 1 thread and all threads"}
     for threads in (1, os.cpu_count() or 1):
         O.set_threads(threads)
         sim = O.Sim(S.dam_break(256), order=2, backend="ref" if kind == "reference" else "oracle")
@@ -326,15 +327,15 @@ def run_ours(args) -> None:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "impl": "ours",
-            "config": config_of(args.cells, world, {"tile": list(args.tile),
-                                                     "min_blocks_per_sm": args.minb,
-                                                     "sim_time_s": c.t, "dt_s": c.dt,
-                                                     **strip_config(args, world)}),
+            "config": config_of(args.cells, world, strip_config(args, world)),
+            "launch": {"tile": list(args.tile), "min_blocks_per_sm": args.minb,
+                       "cells_per_lane": args.tile[1] // 32,
+                       "sim_time_s": c.t, "dt_s": c.dt},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
-                         "kernel": f"rows_step_kernel<float,{args.tile[0]},minb={args.minb}> "
-                                   f"general-tile and all-valid-tile builds, run at once; "
-                                   f"timed together as the step",
+                         "kernel": f"{step_kernel_name(args)} general-tile and "
+                                   f"all-valid-tile builds, run at once; timed together as "
+                                   f"the step",
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "traffic": profiled_traffic()},
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": bytes_io,
@@ -364,8 +365,7 @@ def run_ours(args) -> None:
                 en["over_plain_fp64"] = en["value"] / line["fp64_plain"]["value"]
             line["ensemble"] = en
         if args.coupled and world == 1:
-            line["coupled"] = coupled_rate(dev, args.coupled_cells, tile=tuple(args.tile),
-                                           minb=args.minb)
+            line["coupled"] = coupled_rate(dev, args.coupled_cells)
         if args.adjoint and world == 1:
             line["adjoint"] = adjoint_cost(dev, args.adjoint_cells, args.adjoint_steps)
         if args.cpu_c1 and world == 1:
@@ -379,6 +379,12 @@ def run_ours(args) -> None:
         dist.barrier()
         dist.destroy_process_group()
     del _lib
+
+
+def step_kernel_name(args) -> str:
+    if args.tile[1] == 64:
+        return f"pairs_step_kernel<{args.tile[0]},minb={args.minb or 4}> (two cells per lane)"
+    return f"rows_step_kernel<float,{args.tile[0]},minb={args.minb}>"
 
 
 def strip_config(args, world: int) -> dict:
@@ -395,28 +401,42 @@ def strip_config(args, world: int) -> dict:
                              f"by hb_fused_finish)"}
 
 
-def plain_fp64_rate(d: dict, dev, steps: int = 5, reference_kernels: bool = True,
+def plain_fp64_rate(d: dict, dev, steps: int = 50, reference_kernels: bool = True,
                     order: int = 2) -> dict:
-    """The plain FP64 GPU path: the reference solver loop (Godunov object API,
-    compacted cells, gather-based per-cell fluxes, host syncs per step) on the
-    same catchment, wall-clock per step; with reference_kernels the ops are the
-    reference's own kernels built for sm_100a (baseline/build_ref_cuda.py),
-    else this library's compat ops."""
-    from hipims_b200.solver import Godunov
+    """The plain FP64 GPU path on the same catchment, wall clock per step: the
+    reference's own solver class (HP/SWE_CUDA.py Godunov, unmodified, staged
+    in baseline/_ref by baseline/install_ref_py.py) and its step loop
+    (CHANS-HiPIMS_server.py:246-256: compacted cells, gather-based per-cell
+    fluxes, nonzero / empty_cache / .item() per step), with its 13 extension
+    modules resolved to the reference's own kernels built for sm_100a
+    (reference_kernels; baseline/build_ref_cuda.py) or to this library's
+    drop-in modules.  Where the reference class is not staged, the restated
+    loop of hipims_b200.solver runs instead and `loop` says so."""
+    from baseline import ref_loop
 
-    impl, path = None, "Godunov loop on the compat ops (reference kernel structure), wall clock"
     if reference_kernels:
         from baseline import ref_gpu
 
         if not ref_gpu.available():
             return {"value": None, "unavailable": "baseline/_ref not built"}
-        impl = ref_gpu.RefGpuOps()
-        path = ("Godunov loop on the reference's own kernels built for sm_100a "
-                "(flux, fluxMask, friction-update, timeControl, station rain), torch.min, "
-                "wall clock")
-    g = Godunov(dev, d["dx"], d["cfl"], 1.0e30, secondOrder=order == 2,
-                firstTimeStep=d["first_dt"], tensorType=torch.float64, ops_impl=impl)
-    g._export_enabled = False
+    kernels = ("the reference's own kernels built for sm_100a (flux, fluxMask, friction-update, "
+               "timeControl, station rain)" if reference_kernels
+               else "this library's drop-in op modules (compat kernels)")
+    if ref_loop.available():
+        mods = ref_loop.reference_kernel_modules() if reference_kernels else ref_loop.b200_modules()
+        cls = ref_loop.load_swe_cuda(mods).Godunov
+        loop = "reference HP/SWE_CUDA.py Godunov, unmodified"
+        kw = {}
+    else:
+        from hipims_b200.solver import Godunov as cls
+
+        loop = "restated Godunov (hipims_b200.solver): the reference class is not staged"
+        kw = {"ops_impl": __import__("baseline.ref_gpu", fromlist=["RefGpuOps"]).RefGpuOps()
+              if reference_kernels else None}
+    g = cls(dev, d["dx"], d["cfl"], 1.0e30, secondOrder=order == 2, firstTimeStep=d["first_dt"],
+            tensorType=torch.float64, **kw)
+    if hasattr(g, "_export_enabled"):
+        g._export_enabled = False
     T = lambda a: torch.as_tensor(np.asarray(a, dtype=np.float64))
     mask = torch.as_tensor(d["mask"])
     g.init__fluidField_tensor(mask, T(d["h"]), T(d["qx"]), T(d["qy"]), T(d["wl"]), T(d["z"]),
@@ -430,17 +450,22 @@ def plain_fp64_rate(d: dict, dev, steps: int = 5, reference_kernels: bool = True
         g.addStation_PrecipitationSource(d["rain"], dev)
         g.time_friction_euler_update_cuda(dev)
 
-    for _ in range(SPINUP):
-        one()
-    torch.cuda.synchronize(dev)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        one()
-    torch.cuda.synchronize(dev)
-    el = time.perf_counter() - t0
+    import contextlib
+    import io
+
+    # the reference's 1st-order addFlux prints t every step: kept, but not on stdout
+    with contextlib.redirect_stdout(io.StringIO()):
+        for _ in range(SPINUP):
+            one()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            one()
+        torch.cuda.synchronize(dev)
+        el = time.perf_counter() - t0
     n = int(g._h_internal.numel())
     return {"value": n * steps / el / 1e9, "unit": METRIC, "steps": steps, "dtype": "f64",
-            "path": path}
+            "loop": loop, "kernels": kernels, "path": f"{loop} on {kernels}, wall clock"}
 
 
 def first_order_rates(d: dict, dev, args, flush: torch.Tensor, stream, steps: int = 500) -> dict:
@@ -452,7 +477,7 @@ def first_order_rates(d: dict, dev, args, flush: torch.Tensor, stream, steps: in
     from hipims_b200.scenarios import catchment_from
 
     fs = FusedSolver(catchment_from(d), dtype=torch.float32, tile=(32, 32), device=dev,
-                     minb=args.minb, order=1)
+                     minb=5, order=1)
     n = sum(i.n_valid for i in fs.inst)
     fs.step(SPINUP + args.warmup)
     torch.cuda.synchronize(dev)
@@ -714,8 +739,11 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cells", type=int, default=N_CELLS)
-    ap.add_argument("--tile", type=int, nargs=2, default=[32, 32])
-    ap.add_argument("--minb", type=int, default=5)
+    ap.add_argument("--tile", type=int, nargs=2, default=[32, 64],
+                    help="tile rows, cols: 32 64 = two cells per lane (default), 32 32 or "
+                         "64 32 = one cell per lane")
+    ap.add_argument("--minb", type=int, default=0,
+                    help="register cap as resident CTAs per SM (0: the build's default)")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-accuracy", dest="accuracy", action="store_false")
@@ -731,8 +759,8 @@ def main() -> None:
     ap.add_argument("--strips", action="store_true",
                     help="one catchment split in row strips over the GPUs (halo exchange) "
                          "instead of independent replicas")
-    ap.add_argument("--cpu-c1", action="store_true",
-                    help="also time the 256^2 dam break on the host (1 and all threads)")
+    ap.add_argument("--no-cpu-c1", dest="cpu_c1", action="store_false",
+                    help="skip the 256^2 dam break timed on the host (1 and all threads)")
     ap.add_argument("--coupled-cells", type=int, default=8192)
     ap.add_argument("--adjoint-cells", type=int, default=1024)
     ap.add_argument("--adjoint-steps", type=int, default=2000)

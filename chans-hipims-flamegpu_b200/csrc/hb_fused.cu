@@ -37,6 +37,7 @@
 
 #include "hb_common.cuh"
 #include "hb_datum_halo.cuh"
+#include "hb_once.h"
 #include "hb_physics.cuh"
 #include "hipims_b200_fused.h"
 
@@ -1568,6 +1569,10 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
               fwd(in.halo_up, in.halo_up_rows + HB_PAD_Y + ry);
             if (ry >= in.rows - HB_PAD_Y && in.halo_down[0] != nullptr)
               fwd(in.halo_down, ry - in.rows + HB_PAD_Y);
+            // the neighbour may be a peer GPU: order these stores system-wide
+            // before this tile's partial, its group count and everything the
+            // host orders after the step (the clock all_reduce)
+            __threadfence_system();
           }
           hmaxg[go] = fmax(h, s.hmax[i * kTW + j]);
           if (h > hs) {
@@ -1641,6 +1646,9 @@ rows_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restric
   }
 }
 
+// The FP32 2nd-order step with two cells per lane (64-wide tiles).
+#include "hb_pairs.cuh"
+
 // Prepare: rain rate and boundary values at t, counters; the volume at t is
 // summed by prepare_volume_kernel, launched after this one.
 template <typename T>
@@ -1697,22 +1705,36 @@ prepare_volume_kernel(const hb_instance *__restrict__ insts) {
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
+// The dynamic shared-memory limit of a kernel, set once per device (the
+// attribute belongs to the kernel on the current device).
+PerDeviceOnce g_smem_attr;
+
+int set_smem_attr(const void *fn, int bytes) {
+  int dev = 0;
+  const cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return set_error(HB_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+  return g_smem_attr.run(dev, fn, [&]() -> int {
+    const cudaError_t a = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               bytes);
+    if (a != cudaSuccess)
+      return set_error(HB_ERR_CUDA, "fused step setup: %s", cudaGetErrorString(a));
+    return (int)HB_OK;
+  });
+}
+
 template <typename T, int TY, int TX, bool FAST = (sizeof(T) == 4)>
 int launch_steps(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   using S = Smem<T, TY, TX>;
-  static std::once_flag once;
-  static cudaError_t attr_err = cudaSuccess;
-  static int blocks_per_sm = 1;
-  std::call_once(once, [] {
-    attr_err = cudaFuncSetAttribute(fused_step_kernel<T, TY, TX, FAST>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(S));
-    if (attr_err == cudaSuccess)
-      attr_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &blocks_per_sm, fused_step_kernel<T, TY, TX, FAST>, kNT, sizeof(S));
-    if (blocks_per_sm < 1) blocks_per_sm = 1;
-  });
-  if (attr_err != cudaSuccess)
-    return set_error(HB_ERR_CUDA, "fused step setup: %s", cudaGetErrorString(attr_err));
+  const void *fn = reinterpret_cast<const void *>(fused_step_kernel<T, TY, TX, FAST>);
+  int rc = set_smem_attr(fn, (int)sizeof(S));
+  if (rc) return rc;
+  int blocks_per_sm = 1;
+  const cudaError_t oe =
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, fused_step_kernel<T, TY, TX, FAST>,
+                                                    kNT, sizeof(S));
+  if (oe != cudaSuccess)
+    return set_error(HB_ERR_CUDA, "fused step setup: %s", cudaGetErrorString(oe));
+  if (blocks_per_sm < 1) blocks_per_sm = 1;
   int grid = b->grid_blocks > 0 ? b->grid_blocks : blocks_per_sm * num_sms();
   if (grid > b->n_tiles) grid = b->n_tiles;
   TilePartial *parts = reinterpret_cast<TilePartial *>(b->workspace);
@@ -1730,7 +1752,7 @@ int launch_steps(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
 // cell is out of its reach; the rows kernel runs those tiles in its all-valid
 // build and the others in its general build.
 // ---------------------------------------------------------------------------
-template <int TY>
+template <int TY, int TW>
 __global__ void __launch_bounds__(kRowsNT)
 classify_tiles_kernel(const hb_instance *__restrict__ insts, const int32_t *__restrict__ tile_inst,
                       int n_tiles, uint8_t *__restrict__ flags) {
@@ -1739,12 +1761,12 @@ classify_tiles_kernel(const hb_instance *__restrict__ insts, const int32_t *__re
   const hb_instance &in = insts[tile_inst[tile]];
   const int lt = tile - in.tile_begin;
   const int tyi = lt / in.tiles_x, txi = lt - tyi * in.tiles_x;
-  const int y0 = tyi * TY, x0 = txi * kTW;
+  const int y0 = tyi * TY, x0 = txi * TW;
   bool ok = !(in.bug_y >= y0 - 2 && in.bug_y <= y0 + TY + 1 && in.bug_x >= x0 - 4 &&
-              in.bug_x <= x0 + 35);
+              in.bug_x <= x0 + TW + 3);
   // raster row y is code row y + HB_PAD_Y, raster column x code column
   // x + HB_CODE_PAD_X; the region lies inside the padded code array
-  constexpr int W = kTW + 8;
+  constexpr int W = TW + 8;
   for (int k = threadIdx.x; k < (TY + 4) * W; k += kRowsNT) {
     const int y = y0 - 2 + k / W, x = x0 - 4 + k % W;
     const uint8_t c = in.code[(size_t)(y + HB_PAD_Y) * in.code_pitch + (x + HB_CODE_PAD_X)];
@@ -1855,16 +1877,9 @@ int launch_rows_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   constexpr int MINB_A = MINB;
   auto *kg = rows_step_kernel<T, TY, FAST, MINB, SOURCES, 0, ORDER>;
   auto *ka = rows_step_kernel<T, TY, FAST, MINB_A, SOURCES, 1, ORDER>;
-  static std::once_flag once;
-  static cudaError_t attr_err = cudaSuccess;
-  std::call_once(once, [&] {
-    attr_err = cudaFuncSetAttribute(kg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(S));
-    if (attr_err == cudaSuccess)
-      attr_err = cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)sizeof(S));
-  });
-  if (attr_err != cudaSuccess)
-    return set_error(HB_ERR_CUDA, "fused step setup: %s", cudaGetErrorString(attr_err));
+  int rc = set_smem_attr(reinterpret_cast<const void *>(kg), (int)sizeof(S));
+  if (!rc) rc = set_smem_attr(reinterpret_cast<const void *>(ka), (int)sizeof(S));
+  if (rc) return rc;
   // One CTA per tile by default (the block scheduler starts the next tile as
   // soon as a CTA retires, which balances tiles of uneven cost): the general
   // tiles on the side stream, at the highest priority so that the slower
@@ -1904,6 +1919,65 @@ int launch_rows_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
     if (e != cudaSuccess) return set_error(HB_ERR_CUDA, "hb_fused_step join: %s", cudaGetErrorString(e));
   }
   return check_launch("hb_fused_step");
+}
+
+// The two-cells-per-lane step (64 x TY tiles), with the same side-stream
+// scheduling as launch_rows_impl: general tiles on the side stream, all-valid
+// tiles on the caller's stream, both at once.
+// The general build keeps the register cap of 3 CTAs per SM (its ghost-face
+// branches spill under a tighter one); MINB caps the all-valid build.
+template <int TY, int MINB, bool SOURCES>
+int launch_pairs_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
+  using S = PairSmem<TY>;
+  auto *kg = pairs_step_kernel<TY, 3, SOURCES, 0>;
+  auto *ka = pairs_step_kernel<TY, MINB, SOURCES, 1>;
+  int rc = set_smem_attr(reinterpret_cast<const void *>(kg), (int)sizeof(S));
+  if (!rc) rc = set_smem_attr(reinterpret_cast<const void *>(ka), (int)sizeof(S));
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lock(g_side_mu);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxSideDevices ||
+      !g_side[dev].stream)
+    return set_error(HB_ERR_ARG, "hb_fused_step: run hb_fused_prepare on this device first");
+  const SideRes &sr = g_side[dev];
+  const int n = b->n_tiles;
+  int n_general = n;
+  const auto it = g_general_tiles.find(b->workspace);
+  if (it != g_general_tiles.end()) n_general = std::max(it->second, 1);
+  const int grid_a = b->grid_blocks > 0 ? std::min(b->grid_blocks, n) : n;
+  const int grid_g = b->grid_blocks > 0 ? std::min(b->grid_blocks, n) : std::min(n_general, n);
+  char *ws = reinterpret_cast<char *>(b->workspace);
+  TilePartial *parts = reinterpret_cast<TilePartial *>(ws);
+  TilePartial *gparts = reinterpret_cast<TilePartial *>(ws + ws_partials_bytes(b->n_tiles));
+  unsigned *gcount = reinterpret_cast<unsigned *>(ws + ws_gcount_offset(b));
+  const int32_t *order = reinterpret_cast<const int32_t *>(ws + ws_order_offset(b));
+  const int32_t *counts = reinterpret_cast<const int32_t *>(ws + ws_counts_offset(b));
+  BcTable *bct = reinterpret_cast<BcTable *>(ws + ws_bct_offset(b));
+  const CUtensorMap *maps = reinterpret_cast<const CUtensorMap *>(ws + ws_maps_offset(b));
+  for (int k = 0; k < nsteps; k++) {
+    cudaError_t e = cudaEventRecord(sr.fork, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(sr.stream, sr.fork, 0);
+    if (e != cudaSuccess) return set_error(HB_ERR_CUDA, "hb_fused_step fork: %s", cudaGetErrorString(e));
+    kg<<<grid_g, kRowsNT, sizeof(S), sr.stream>>>(b->instances, b->tile_instance, order, counts,
+                                                  parts, gparts, gcount, bct, maps);
+    ka<<<grid_a, kRowsNT, sizeof(S), st>>>(b->instances, b->tile_instance, order, counts, parts,
+                                           gparts, gcount, bct, maps);
+    e = cudaEventRecord(sr.join, sr.stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, sr.join, 0);
+    if (e != cudaSuccess) return set_error(HB_ERR_CUDA, "hb_fused_step join: %s", cudaGetErrorString(e));
+  }
+  return check_launch("hb_fused_step");
+}
+
+int launch_pairs(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
+  const int minb = (b->flags >> HB_FLAG_MINB_SHIFT) & 0xF;
+  const bool src = (b->flags & HB_FLAG_SOURCES) != 0;
+  if (minb == 3) return src ? launch_pairs_impl<32, 3, true>(b, nsteps, st)
+                            : launch_pairs_impl<32, 3, false>(b, nsteps, st);
+  if (minb == 0 || minb == 4) return src ? launch_pairs_impl<32, 4, true>(b, nsteps, st)
+                                         : launch_pairs_impl<32, 4, false>(b, nsteps, st);
+  return set_error(HB_ERR_ARG, "hb_fused_step: 64-wide tiles are built for 3 or 4 CTAs per SM "
+                               "(minb 0, 3 or 4), not %d", minb);
 }
 
 // The build with the infiltration / station-rain branches when the batch
@@ -1961,6 +2035,7 @@ int encode_2d(CUtensorMap *map, CUtensorMapDataType dt, size_t esize, const void
 int encode_maps(const hb_fused_batch *b, cudaStream_t st, CUtensorMap *host_maps) {
   if (!b->instances_host) return set_error(HB_ERR_ARG, "hb_fused_prepare: instances_host is null");
   const int TY = b->tile_y;
+  const int TW = b->tile_x;  // 32 (rows kernel) or 64 (two cells per lane)
   const size_t es = b->dtype == HB_F64 ? 8 : 4;
   const CUtensorMapDataType dt =
       b->dtype == HB_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
@@ -1969,18 +2044,19 @@ int encode_maps(const hb_fused_batch *b, cudaStream_t st, CUtensorMap *host_maps
   for (int i = 0; i < b->n_instances; i++) {
     const hb_instance &in = b->instances_host[i];
     const uint64_t rows_s = (uint64_t)((in.rows + 63) / 64 * 64 + 2 * HB_PAD_Y);
-    if ((int64_t)in.tiles_y * TY + 4 > (int64_t)rows_s || in.tiles_x * kTW + 8 > in.pitch)
+    if ((int64_t)in.tiles_y * TY + 4 > (int64_t)rows_s || in.tiles_x * TW + 8 > in.pitch ||
+        in.tiles_x * TW + 32 > in.code_pitch)
       return set_error(HB_ERR_ARG, "instance %d: storage smaller than its tiles", i);
     CUtensorMap *m = &maps[(size_t)i * kMapsPerInstance];
     const void *srcs[7] = {in.h[0], in.h[1], in.qx[0], in.qx[1], in.qy[0], in.qy[1], in.z};
     for (int k = 0; k < 7; k++) {
-      int rc = encode_2d(&m[k], dt, es, srcs[k], (uint64_t)in.pitch, rows_s, kSWF, TY + 4);
+      int rc = encode_2d(&m[k], dt, es, srcs[k], (uint64_t)in.pitch, rows_s, TW + 8, TY + 4);
       if (rc) return rc;
     }
-    int rc = encode_2d(&m[7], dt, es, in.h_max, (uint64_t)in.pitch, rows_s, kTW, TY);
+    int rc = encode_2d(&m[7], dt, es, in.h_max, (uint64_t)in.pitch, rows_s, TW, TY);
     if (rc) return rc;
     rc = encode_2d(&m[8], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, in.code, (uint64_t)in.code_pitch,
-                   rows_s, kSWC, TY + 4);
+                   rows_s, TW + 32, TY + 4);
     if (rc) return rc;
   }
   char *dst = reinterpret_cast<char *>(b->workspace) + ws_maps_offset(b);
@@ -2012,8 +2088,13 @@ int prepare_impl(const hb_fused_batch *b, cudaStream_t st, CUtensorMap *host_map
   if (b->dtype != HB_F32 && b->dtype != HB_F64)
     return set_error(HB_ERR_ARG, "hb_fused_prepare: bad dtype %d", b->dtype);
   if (uses_rows_kernel(b)) {
-    if (b->tile_x != kTW || (b->tile_y != 32 && b->tile_y != 64))
-      return set_error(HB_ERR_ARG, "hb_fused_prepare: rows kernel tiles are 32 wide, 32 or 64 high");
+    const bool pairs = b->tile_x == kPW && b->tile_y == 32;
+    if (!pairs && (b->tile_x != kTW || (b->tile_y != 32 && b->tile_y != 64)))
+      return set_error(HB_ERR_ARG, "hb_fused_prepare: rows kernel tiles are 32 wide, 32 or 64 "
+                                   "high, or 64 wide and 32 high");
+    if (pairs && (b->dtype != HB_F32 || b->order != 2 || (b->flags & HB_FLAG_EXACT_FP32)))
+      return set_error(HB_ERR_ARG, "hb_fused_prepare: 64-wide tiles (two cells per lane) are "
+                                   "built for the FP32 2nd-order step");
     int rc;
     if (host_maps) {
       rc = encode_maps(b, st, host_maps);
@@ -2053,12 +2134,15 @@ int prepare_impl(const hb_fused_batch *b, cudaStream_t st, CUtensorMap *host_map
     if (rc) return rc;
     char *ws = reinterpret_cast<char *>(b->workspace);
     uint8_t *flags = reinterpret_cast<uint8_t *>(ws + ws_flags_offset(b));
-    if (b->tile_y == 64)
-      classify_tiles_kernel<64><<<b->n_tiles, kRowsNT, 0, st>>>(b->instances, b->tile_instance,
-                                                                 b->n_tiles, flags);
+    if (b->tile_x == kPW)
+      classify_tiles_kernel<32, kPW><<<b->n_tiles, kRowsNT, 0, st>>>(
+          b->instances, b->tile_instance, b->n_tiles, flags);
+    else if (b->tile_y == 64)
+      classify_tiles_kernel<64, kTW><<<b->n_tiles, kRowsNT, 0, st>>>(
+          b->instances, b->tile_instance, b->n_tiles, flags);
     else
-      classify_tiles_kernel<32><<<b->n_tiles, kRowsNT, 0, st>>>(b->instances, b->tile_instance,
-                                                                 b->n_tiles, flags);
+      classify_tiles_kernel<32, kTW><<<b->n_tiles, kRowsNT, 0, st>>>(
+          b->instances, b->tile_instance, b->n_tiles, flags);
     order_tiles_kernel<<<1, kOrderNT, 0, st>>>(
         flags, b->n_tiles, reinterpret_cast<int32_t *>(ws + ws_order_offset(b)),
         reinterpret_cast<int32_t *>(ws + ws_counts_offset(b)));
@@ -2138,6 +2222,11 @@ extern "C" int hb_fused_step(const hb_fused_batch *b, int nsteps, void *stream) 
     return set_error(HB_ERR_ARG, "hb_fused_step: order 1 is built for 32 x 32 tiles, FP32 (fast, "
                                  "minb 0 or 5) and FP64");
   }
+  if (uses_rows_kernel(b) && tx == kPW) {
+    if (ty == 32 && b->dtype == HB_F32 && !exact && b->order == 2) return launch_pairs(b, nsteps, st);
+    return set_error(HB_ERR_ARG, "hb_fused_step: 64-wide tiles are built for the FP32 2nd-order "
+                                 "step with 32-row tiles");
+  }
   if (uses_rows_kernel(b)) {
     if (tx != kTW) return set_error(HB_ERR_ARG, "hb_fused_step: rows kernel tiles are 32 wide");
     if (b->dtype == HB_F32 && exact) {
@@ -2173,9 +2262,14 @@ extern "C" int hb_fused_step(const hb_fused_batch *b, int nsteps, void *stream) 
 // in g_noalloc_scratch, kNoAllocScratchBytes per GPU that loads the library,
 // held until the process exits.  Host code must not pass g_noalloc_scratch to
 // a kernel directly: in host code that name is only a stand-in for the device
-// symbol.  Its device address is looked up once per device with
-// cudaGetSymbolAddress (on the first call on that device, which is why that
-// first call should come before any stream capture) and cached.
+// symbol.  Its device address is looked up with cudaGetSymbolAddress on the
+// current device by every call with prepare != 0 (so a call after
+// cudaDeviceReset that prepares picks up the new address) and kept for the
+// calls without prepare.  The first prepare on a device also creates the side
+// stream, which is why that call should come before any stream capture.
+// The identity of the batch last prepared is kept per device too, so that a
+// call without prepare for another batch is refused instead of running on
+// that batch's tensor maps, tile order and counts.
 // ---------------------------------------------------------------------------
 namespace hb {
 namespace {
@@ -2186,8 +2280,35 @@ constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
+// What a prepared scratch belongs to: a prepare == 0 call must present the
+// same batch.
+struct NoAllocOwner {
+  bool valid = false;
+  const void *instances = nullptr;
+  const void *tile_instance = nullptr;
+  int32_t n_tiles = 0, n_instances = 0, tile_y = 0, tile_x = 0, dtype = 0, order = 0, flags = 0;
+  bool same(const hb_fused_batch *b) const {
+    return valid && instances == b->instances && tile_instance == b->tile_instance &&
+           n_tiles == b->n_tiles && n_instances == b->n_instances && tile_y == b->tile_y &&
+           tile_x == b->tile_x && dtype == b->dtype && order == b->order && flags == b->flags;
+  }
+  void set(const hb_fused_batch *b) {
+    valid = true;
+    instances = b->instances;
+    tile_instance = b->tile_instance;
+    n_tiles = b->n_tiles;
+    n_instances = b->n_instances;
+    tile_y = b->tile_y;
+    tile_x = b->tile_x;
+    dtype = b->dtype;
+    order = b->order;
+    flags = b->flags;
+  }
+};
+
 std::mutex g_noalloc_mu;
 void *g_noalloc_ptr[kMaxDevices];
+NoAllocOwner g_noalloc_owner[kMaxDevices];
 // host staging of the tensor maps (no heap allocation on this path)
 CUtensorMap g_noalloc_maps[kNoAllocMaxInstances * kMapsPerInstance];
 
@@ -2215,18 +2336,26 @@ extern "C" int hb_fused_step_noalloc(const hb_fused_batch *b, int nsteps, int pr
   if (e != cudaSuccess) return set_error(HB_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices)
     return set_error(HB_ERR_LIMIT, "hb_fused_step_noalloc: device %d out of range", dev);
-  if (!g_noalloc_ptr[dev]) {
+  NoAllocOwner &owner = g_noalloc_owner[dev];
+  if (prepare) {
     void *p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p)
       return set_error(HB_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
     g_noalloc_ptr[dev] = p;
+    owner.valid = false;  // the scratch is being rewritten
+    local.workspace = p;
+    int rc = prepare_impl(&local, as_stream(stream), g_noalloc_maps);
+    if (rc) return rc;
+    owner.set(b);
+  } else if (!owner.same(b)) {
+    return set_error(HB_ERR_ARG,
+                     owner.valid ? "hb_fused_step_noalloc: the fixed scratch on device %d was "
+                                   "last prepared for another batch; call with prepare != 0"
+                                 : "hb_fused_step_noalloc: the fixed scratch on device %d has not "
+                                   "been prepared; call with prepare != 0 first",
+                     dev);
   }
   local.workspace = g_noalloc_ptr[dev];
-  auto st = as_stream(stream);
-  if (prepare) {
-    int rc = prepare_impl(&local, st, g_noalloc_maps);
-    if (rc) return rc;
-  }
   return hb_fused_step(&local, nsteps, stream);
 }

@@ -206,7 +206,11 @@ class FusedSolver:
 
     order 2 (default): the reference's 2nd-order scheme (MUSCL, `secondOrder`
     True); order 1: its 1st-order scheme (`secondOrder` False, the coupled
-    server's choice, CHANS-HiPIMS_server.py), rows kernel with 32 x 32 tiles."""
+    server's choice, CHANS-HiPIMS_server.py), rows kernel with 32 x 32 tiles.
+
+    tile = (rows, cols): (32, 64) runs two cells per lane (FP32 2nd order, the
+    default there); (32, 32) and (64, 32) one cell per lane (every dtype and
+    order)."""
 
     def __init__(self, catchments: Catchment | Sequence[Catchment], dtype=torch.float32,
                  tile: tuple[int, int] | None = None, device="cuda", grid_blocks: int = 0,
@@ -223,9 +227,11 @@ class FusedSolver:
         self.device = torch.device(device)
         self.dtype = dtype
         self.order = order
-        if tile is None:  # rows kernel: 32 wide; 64 high in FP32 order 2, else 32 high
-            tile = (64, 32) if dtype == torch.float32 and kernel == "rows" and order == 2 \
-                else (32, 32)
+        if tile is None:
+            # FP32 2nd order (not exact_fp32): 32 x 64 tiles, two cells per lane;
+            # otherwise the 32 x 32 row-walking tiles
+            pairs = dtype == torch.float32 and kernel == "rows" and order == 2 and not exact_fp32
+            tile = (32, 64) if pairs else (32, 32)
         self.tile = tuple(tile)
         self.inst = [_Instance(c, dtype, self.device, self.tile) for c in catchments]
         n = len(self.inst)

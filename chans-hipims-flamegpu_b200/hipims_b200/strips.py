@@ -29,9 +29,11 @@ DistributedStrips) folds step 1 into step 2: the step kernel stores the new
 state of each strip's first and last two rows also into the neighbour's halo
 rows of the same output buffer (hb_instance.halo_up / halo_down), which no
 kernel reads during that step.  Across ranks the neighbour's arrays are mapped
-with CUDA IPC, the stores are plain peer stores, and the clock all_reduce that
-follows every step orders them before the neighbour's next step.  One exchange
-at start-up fills the halos of the initial state.
+with CUDA IPC, the stores are plain peer stores, each thread that made them
+issues a system-scope fence (__threadfence_system) before the tile's partial
+sum and count, and the clock all_reduce that follows every step orders them
+before the neighbour's next step.  One exchange at start-up fills the halos of
+the initial state.
 """
 from __future__ import annotations
 

@@ -94,8 +94,8 @@ def sim_steps(sim):
     return getattr(sim, "_steps", 0)
 
 
-@pytest.mark.parametrize("tile,kernel", [((64, 32), "rows"), ((32, 32), "rows"),
-                                         ((32, 32), "tasks")])
+@pytest.mark.parametrize("tile,kernel", [((32, 64), "rows"), ((64, 32), "rows"),
+                                         ((32, 32), "rows"), ((32, 32), "tasks")])
 def test_fused_fp32_dam_break_1000_steps(cuda, tile, kernel):
     """Config 1 (256 x 256, 1000 steps) in FP32 vs the FP64 oracle at the
     same simulated times.  The problem is uniform along y, so qy must stay
@@ -164,18 +164,19 @@ def test_fused_batch_equals_single_runs(cuda):
         assert fb.controls()[k].t == f1.controls()[0].t
 
 
-def test_fused_persistent_grid_equals_one_block_per_tile(cuda):
+@pytest.mark.parametrize("tile", [(32, 32), (32, 64)])
+def test_fused_persistent_grid_equals_one_block_per_tile(cuda, tile):
     """A few CTAs looping over every tile of a batch (grid_blocks > 0) against
     the default of one CTA per tile: the per-tile partials and the fixed-order
     group sums make fields, clocks and volumes identical, bit for bit.  The
-    400 x 400 catchment has 169 tiles, so two reduction groups."""
+    400 x 400 catchment has 169 (32 x 32) or 91 (32 x 64) tiles."""
     from hipims_b200 import scenarios as S
     from hipims_b200.fused import FusedSolver
 
     ds = [S.urban_catchment(n, seed=k + 20, rain_mm_h=100.0) for k, n in enumerate((400, 70, 130))]
     cs = [catchment(d) for d in ds]
-    a = FusedSolver(cs, dtype=torch.float32, device=cuda, tile=(32, 32))
-    b = FusedSolver(cs, dtype=torch.float32, device=cuda, tile=(32, 32), grid_blocks=7)
+    a = FusedSolver(cs, dtype=torch.float32, device=cuda, tile=tile)
+    b = FusedSolver(cs, dtype=torch.float32, device=cuda, tile=tile, grid_blocks=7)
     a.step(40)
     b.step(40)
     for k in range(len(cs)):
