@@ -108,7 +108,10 @@ int hb_infiltration(int dtype, int64_t M, const int32_t *wet_mask, void *h_updat
 
 /* Device-side minimum of x[0..M) written to out[0] -- replaces the
  * torch.min(accelerator) of HP/SWE_CUDA.py:818-820 without a host sync.
- * workspace: hb_min_reduce_workspace_size(M) bytes, or NULL when M <= 4096. */
+ * workspace: hb_min_reduce_workspace_size(M) bytes, or NULL when M <= 4096;
+ * zero-filled before its first use.  Every call leaves it ready for the next
+ * (its first word, a block counter, is back at zero), so one workspace of the
+ * largest size needed serves calls of any size ordered on one stream. */
 size_t hb_min_reduce_workspace_size(int64_t M);
 int hb_min_reduce(int dtype, int64_t M, const void *x, void *out, void *workspace,
                   void *stream);
@@ -156,11 +159,18 @@ int hb_fused_finish(const struct hb_fused_batch *batch, const double *ext, void 
  *  - Limits: hb_fused_workspace_size(b) <= 4 MiB (about 110,000 tiles, e.g.
  *    110 M cells with 32 x 32 tiles; about 100,000 with 256 instances) and at
  *    most 256 instances; larger batches get HB_ERR_LIMIT with a message.
- *  - The first call on a device looks up the array's device address, and the
- *    first call with prepare != 0 on a device creates the library's side
- *    stream and two events for that device (kept until exit; no device
- *    memory is allocated for them by this library); make that first call
- *    before any stream capture.
+ *  - Every call with prepare != 0 looks up the array's device address on the
+ *    current device, and the first such call on a device creates the
+ *    library's side stream and two events for that device (kept until exit;
+ *    no device memory is allocated for them by this library); make that
+ *    first call before any stream capture.  After cudaDeviceReset the array
+ *    has a new address: the next call on that device must pass prepare != 0.
+ *  - The library remembers, per device, which batch the array was last
+ *    prepared for (its instance records, tile and instance counts, tile
+ *    shape, dtype, order and flags).  A call with prepare == 0 for any other
+ *    batch, or before any prepare on that device, returns HB_ERR_ARG instead
+ *    of running with another batch's scratch.  Two batches used in turn each
+ *    need prepare != 0 when their turn comes.
  *  - Every call on a device shares the one array and leaves its contents
  *    behind: calls that overlap on the GPU (other streams, other threads)
  *    race with each other. */

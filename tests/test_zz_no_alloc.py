@@ -51,6 +51,75 @@ def test_noalloc_matches_workspace_entry_over_two_calls(cuda):
     _compare(a, b)
 
 
+def _solvers(cuda, sizes, seed):
+    from hipims_b200 import scenarios as S
+    from hipims_b200.fused import FusedSolver
+    from hipims_b200.scenarios import catchment_from
+
+    cs = [catchment_from(S.urban_catchment(n, seed=seed + k, rain_mm_h=200.0))
+          for k, n in enumerate(sizes)]
+    return (FusedSolver(cs, dtype=torch.float32, device=cuda),
+            FusedSolver(cs, dtype=torch.float32, device=cuda))
+
+
+def _compare_all(a, b):
+    torch.cuda.synchronize()
+    for k in range(len(a.inst)):
+        ca, cb = a.controls()[k], b.controls()[k]
+        assert ca.step == cb.step and ca.t == cb.t and ca.dt == cb.dt
+        sa, sb = a.compacted(k), b.compacted(k)
+        for f in ("h", "qx", "qy", "h_max"):
+            assert np.abs(sa[f] - sb[f]).max() <= TOL, (k, f)
+
+
+def test_noalloc_two_batches_in_turn(cuda):
+    """Batch A, then batch B of another size and instance count (other tile
+    counts, workspace offsets and tile order in the shared array), then A
+    again: each call re-prepares the array for its batch and matches that
+    batch's workspace twin."""
+    a_ws, a_na = _solvers(cuda, (150,), 3)
+    b_ws, b_na = _solvers(cuda, (90, 200), 11)
+    for steps in (6, 4):
+        a_ws.step(steps)
+        a_na.step_noalloc(steps, prepare=True)
+        _compare_all(a_ws, a_na)
+        b_ws.step(steps)
+        b_na.step_noalloc(steps, prepare=True)
+        _compare_all(b_ws, b_na)
+    a_ws.step(3)
+    a_na.step_noalloc(3, prepare=True)
+    _compare_all(a_ws, a_na)
+    a_ws.step(2)
+    a_na.step_noalloc(2)  # A was prepared last: no prepare needed
+    _compare_all(a_ws, a_na)
+
+
+def test_noalloc_refuses_a_batch_it_was_not_prepared_for(cuda):
+    """A call without prepare for a batch other than the one the array was
+    last prepared for returns HB_ERR_ARG and leaves that batch's state alone."""
+    import ctypes
+
+    from hipims_b200 import _lib
+
+    a_ws, a_na = _solvers(cuda, (120,), 5)
+    _, b_na = _solvers(cuda, (80,), 7)
+    a_na.step_noalloc(2, prepare=True)
+    before = b_na.compacted(0)["h"].copy()
+    L = _lib.lib()
+    with torch.cuda.device(cuda):
+        rc = L.hb_fused_step_noalloc(ctypes.byref(b_na.batch), 1, 0,
+                                     torch.cuda.current_stream(cuda).cuda_stream)
+    assert rc == -1
+    assert b"another batch" in L.hb_last_error()
+    torch.cuda.synchronize()
+    assert b_na.controls()[0].step == 0
+    np.testing.assert_array_equal(b_na.compacted(0)["h"], before)
+    # the array still belongs to A: A continues without a prepare
+    a_ws.step(3)
+    a_na.step_noalloc(1)
+    _compare_all(a_ws, a_na)
+
+
 def test_noalloc_rejects_batches_beyond_its_scratch(cuda):
     import ctypes
 
