@@ -544,16 +544,18 @@ extern "C" int hb_min_reduce(int dtype, int64_t M, const void *x, void *out, voi
   if (nb > kMinMaxBlocks) nb = kMinMaxBlocks;
   HB_REQUIRE(nb == 1 || workspace, "hb_min_reduce: workspace required for M=%lld",
              (long long)M);
-  unsigned int *counter =
-      nb == 1 ? nullptr
-              : (unsigned int *)((char *)workspace + (size_t)nb * sizeof(double) + 128);
+  // the block counter sits at a fixed offset (the first word) so that a
+  // workspace reused for inputs of other sizes finds it where the last call
+  // left it (zero); the block partials follow at 256 bytes
+  unsigned int *counter = nb == 1 ? nullptr : (unsigned int *)workspace;
+  void *partial = nb == 1 ? nullptr : (void *)((char *)workspace + 256);
   auto s = as_stream(stream);
   if (dtype == HB_F64)
     min_reduce_kernel<double><<<(unsigned)nb, kMinThreads, 0, s>>>(
-        M, (const double *)x, (double *)out, (double *)workspace, counter);
+        M, (const double *)x, (double *)out, (double *)partial, counter);
   else
     min_reduce_kernel<float><<<(unsigned)nb, kMinThreads, 0, s>>>(
-        M, (const float *)x, (float *)out, (float *)workspace, counter);
+        M, (const float *)x, (float *)out, (float *)partial, counter);
   return check_launch("hb_min_reduce");
 }
 

@@ -18,6 +18,8 @@ are checked and CUDA launch errors raise instead of being printed.
 """
 from __future__ import annotations
 
+import threading
+
 import torch
 
 from . import _lib
@@ -208,15 +210,35 @@ def infiltration(wetMask, h_update, landuse, h, hydraulic_conductivity, capillar
     _lib.check(rc, "addinfiltration")
 
 
+# hb_min_reduce workspaces, one per (device, stream), grown on demand: the
+# kernel leaves its block counter at zero after every call, so a workspace is
+# zero-filled once, when it is allocated, and calls ordered on one stream can
+# share it.
+_MIN_WS: dict = {}
+_MIN_WS_LOCK = threading.Lock()
+
+
+def _min_workspace(x: torch.Tensor, nbytes: int) -> torch.Tensor:
+    key = (x.device.index, _stream(x))
+    with _MIN_WS_LOCK:
+        ws = _MIN_WS.get(key)
+        if ws is None or ws.numel() < nbytes:
+            ws = torch.zeros(nbytes, dtype=torch.uint8, device=x.device)
+            _MIN_WS[key] = ws
+        return ws
+
+
 def device_min(x: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
-    """min(x) on the device without a host sync (replaces torch.min(accelerator))."""
+    """min(x) on the device without a host sync (replaces torch.min(accelerator)).
+    Allocates nothing per call once its per-stream workspace has grown to the
+    largest size seen."""
     _check_input("x", x)
     dtype = _dtype_of(x, {})
     if out is None:
         out = torch.empty(1, dtype=x.dtype, device=x.device)
     L = _lib.lib()
     nbytes = L.hb_min_reduce_workspace_size(x.numel())
-    ws = torch.zeros(max(nbytes, 1), dtype=torch.uint8, device=x.device) if nbytes else None
+    ws = _min_workspace(x, nbytes) if nbytes else None
     with torch.cuda.device(x.device):
         rc = L.hb_min_reduce(dtype, x.numel(), _p(x), _p(out), _p(ws) if ws is not None else None,
                              _stream(x))
