@@ -26,7 +26,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_ref")
 LIB = os.path.join(OUT_DIR, "libhipims_ref_cuda.so")
-DEFAULT_REF = "/root/reference"
+# the reference checkout: $HIPIMS_REFERENCE_ROOT, else where this recipe was written
+DEFAULT_REF = os.environ.get("HIPIMS_REFERENCE_ROOT", "/root/reference")
 KERNEL_DIR = os.path.join("CHANS-HiPIMS", "hipims", "cuda")
 
 _LAUNCH = {

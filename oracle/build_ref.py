@@ -25,7 +25,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_ref")
 LIB = os.path.join(OUT_DIR, "libhipims_ref_host.so")
-DEFAULT_REF = "/root/reference"
+# the reference checkout: $HIPIMS_REFERENCE_ROOT, else where this recipe was written
+DEFAULT_REF = os.environ.get("HIPIMS_REFERENCE_ROOT", "/root/reference")
 KERNEL_DIR = os.path.join("CHANS-HiPIMS", "hipims", "cuda")
 
 # Host drivers: one extern "C" entry per kernel.  Each loops over the kernel's
