@@ -46,7 +46,26 @@ def _entry(tag: int, typ: int, values) -> tuple[int, int, int, bytes]:
     return tag, typ, len(values), struct.pack("<" + fmt * len(values), *values)
 
 
-def _geo_entries(transform, epsg: int | None, geographic: bool | None) -> list:
+def _raw_geokey_entries(geokeys: dict) -> list:
+    """GeoKeyDirectory (34735), GeoDoubleParams (34736) and GeoAsciiParams
+    (34737) copied as read from another GeoTIFF: a CRS that is not one EPSG
+    code (a user-defined projection, a datum given by parameters) passes
+    through unchanged."""
+    out = []
+    if 34735 in geokeys:
+        out.append(_entry(34735, _SHORT, [int(v) for v in geokeys[34735]]))
+    if 34736 in geokeys:
+        out.append(_entry(34736, _DOUBLE, [float(v) for v in geokeys[34736]]))
+    if 34737 in geokeys:
+        txt = geokeys[34737]
+        if isinstance(txt, bytes):
+            txt = txt.decode("ascii", "replace")
+        out.append(_entry(34737, _ASCII, str(txt).rstrip("\0")))
+    return out
+
+
+def _geo_entries(transform, epsg: int | None, geographic: bool | None,
+                 geokeys: dict | None = None) -> list:
     out = []
     if transform is not None:
         t = [float(v) for v in transform]
@@ -61,6 +80,8 @@ def _geo_entries(transform, epsg: int | None, geographic: bool | None) -> list:
         else:
             out.append(_entry(34264, _DOUBLE, (a, b, 0.0, c, d, e, 0.0, f,  # ModelTransformation
                                                0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0)))
+    if geokeys:
+        return out + _raw_geokey_entries(geokeys)
     keys = []
     if epsg is not None:
         geo = (int(epsg) in GEOGRAPHIC_EPSG) if geographic is None else bool(geographic)
@@ -79,10 +100,13 @@ def _geo_entries(transform, epsg: int | None, geographic: bool | None) -> list:
 
 def write_geotiff(path: str, data, transform: Sequence[float] | None = None,
                   epsg: int | None = None, nodata: float | None = -9999.0,
-                  geographic: bool | None = None) -> str:
+                  geographic: bool | None = None, geokeys: dict | None = None) -> str:
     """Write a 2-D array as a single-band float32 GeoTIFF (little-endian,
     uncompressed, one strip).  epsg: the CRS as an EPSG code (a projected CRS
-    unless the code is a known geographic one or `geographic` says so)."""
+    unless the code is a known geographic one or `geographic` says so);
+    geokeys: the GeoKey tags of another GeoTIFF ({34735: ..., 34736: ...,
+    34737: ...}, as read_geotiff returns them in meta["geokeys"]), written
+    verbatim instead."""
     arr = np.ascontiguousarray(np.asarray(data), dtype="<f4")
     if arr.ndim != 2:
         raise ValueError("write_geotiff: a 2-D raster")
@@ -97,7 +121,7 @@ def write_geotiff(path: str, data, transform: Sequence[float] | None = None,
         _entry(277, _SHORT, [1]), _entry(278, _LONG, [rows]), _entry(279, _LONG, [nbytes]),
         _entry(284, _SHORT, [1]), _entry(339, _SHORT, [3]),
     ]
-    entries += _geo_entries(transform, epsg, geographic)
+    entries += _geo_entries(transform, epsg, geographic, geokeys)
     if nodata is not None:
         entries.append(_entry(42113, _ASCII, "%.17g" % float(nodata)))  # GDAL_NODATA
     entries.sort(key=lambda x: x[0])
@@ -137,6 +161,7 @@ def reference_tif_name(pt_path: str) -> str:
 
 def export_raster_tiff(outpath: str, mask, transform: Sequence[float] | None = None,
                        epsg: int | None = None, nodata: float = -9999.0,
+                       geokeys: dict | None = None,
                        pattern: str = "*.pt") -> list[str]:
     """GeoTIFFs of every exported field file in `outpath`
     (`FusedSolver.export_fields`, `Godunov.exportField`): the compacted vector
@@ -153,7 +178,8 @@ def export_raster_tiff(outpath: str, mask, transform: Sequence[float] | None = N
             raise ValueError(f"{p}: {vec.shape[0]} values for {int(valid.sum())} valid cells")
         raster = np.full(valid.shape, nodata, dtype=np.float32)
         raster[valid] = vec.astype(np.float32)
-        out.append(write_geotiff(reference_tif_name(p), raster, transform, epsg, nodata))
+        out.append(write_geotiff(reference_tif_name(p), raster, transform, epsg, nodata,
+                                 geokeys=geokeys))
     return out
 
 
@@ -385,7 +411,8 @@ def _geo_meta(t: dict, width: int, height: int, count: int, dtype) -> dict:
         # the origin half a pixel to the corner
         a, b, c, d_, e, f = transform
         transform = (a, b, c - 0.5 * a - 0.5 * b, d_, e, f - 0.5 * d_ - 0.5 * e)
-    epsg = keys.get(3072) or keys.get(2048)
+    # 32767 marks a user-defined CRS (its parameters are in other keys), not an EPSG code
+    epsg = next((keys[k] for k in (3072, 2048) if keys.get(k) not in (None, 0, 32767)), None)
     nodata = None
     if 42113 in t:
         try:
@@ -398,6 +425,7 @@ def _geo_meta(t: dict, width: int, height: int, count: int, dtype) -> dict:
         xs = [c, c + a * width, c + b * height, c + a * width + b * height]
         ys = [f, f + d_ * width, f + e * height, f + d_ * width + e * height]
         bounds = (min(xs), min(ys), max(xs), max(ys))
+    geokeys = {k: t[k] for k in (34735, 34736, 34737) if k in t}
     return dict(driver="GTiff", dtype=str(np.dtype(dtype)), nodata=nodata, width=width,
                 height=height, count=count, crs=f"EPSG:{epsg}" if epsg else None,
-                transform=transform, bounds=bounds)
+                transform=transform, bounds=bounds, geokeys=geokeys)

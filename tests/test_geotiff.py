@@ -75,3 +75,40 @@ def test_export_raster_tiff_scatters_compacted_fields(tmp_path):
     with pytest.raises(ValueError):
         torch.save(vec[:-1], str(tmp_path / name))
         export_raster_tiff(str(tmp_path), mask)
+
+
+def test_export_keeps_a_crs_that_is_not_an_epsg_code(tmp_path):
+    """A DEM whose CRS is user-defined (ProjectedCSType 32767, parameters in
+    GeoDoubleParams, a citation in GeoAsciiParams): exportRaster_tiff copies
+    the DEM's GeoKey tags into every result raster instead of dropping them."""
+    from hipims_b200.geotiff import read_geotiff
+    from hipims_b200.postprocessing import exportRaster_tiff
+
+    geokeys = {
+        # version 1.1.0, 5 keys: model projected, pixel is area, user-defined
+        # projected CRS, its citation (ascii params 0..), a linear unit (m)
+        34735: [1, 1, 0, 5, 1024, 0, 1, 1, 1025, 0, 1, 1, 3072, 0, 1, 32767,
+                3073, 34737, 24, 0, 3076, 0, 1, 9001],
+        34736: [6378137.0, 298.257223563, 0.9996, 500000.0],
+        34737: "custom transverse merc|",
+    }
+    dem = np.full((5, 6), -9999.0)
+    dem[1:-1, 1:-1] = 3.0
+    dem_path = write_geotiff(str(tmp_path / "dem.tif"), dem,
+                             transform=(2.0, 0.0, 1000.0, 0.0, -2.0, 5000.0), geokeys=geokeys)
+    _, meta = read_geotiff(dem_path)
+    assert meta["crs"] is None and meta["geokeys"][34735] == geokeys[34735]
+    out = tmp_path / "out"
+    out.mkdir()
+    vec = torch.arange(12, dtype=torch.float64)
+    torch.save(vec, str(out / "h_tensor([60.], device='cuda:0', dtype=torch.float64).pt"))
+    paths = exportRaster_tiff(dem_path, str(out))
+    assert paths == [str(out / "h_60.tif")]
+    got, tags = _read(paths[0])
+    assert list(tags[34735]) == geokeys[34735]
+    assert tuple(tags[34736]) == tuple(geokeys[34736])
+    assert tags[34737] == geokeys[34737]
+    assert tuple(tags[33550]) == (2.0, 2.0, 0.0)
+    want = np.full(dem.shape, -9999.0, dtype=np.float32)
+    want[1:-1, 1:-1] = vec.numpy().reshape(3, 4)
+    np.testing.assert_array_equal(got, want)
