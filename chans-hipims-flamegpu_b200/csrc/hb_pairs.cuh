@@ -135,19 +135,30 @@ struct Fc2 {
   f2 fh, fx, fy, sa, sb;
 };
 
-// Two faces in the face frame.  Edge states L (minus side) and R (plus side):
-// depth, bed (measured from the minus cell's bed), normal and tangential
-// discharge; the two cells' depths ah, bh and free-surface levels wa, wb
-// (wa = ah in this frame) and the plus cell's bed bz.  Velocities are taken
-// from the edge states, then the hydrostatic step
-// (HC/flucCal_2ndOrder_jh_improved_Kernel.cu:43-72), the HLLC flux (:109-195,
-// with the single-precision shortcuts of hllc<float, true>) and the two
-// bed-slope terms (:494-501).  fn / ft: normal / tangential momentum flux; ft
-// is linear in the tangential discharge, so a caller that passes +q instead
-// of -q for it takes -ft.
-__device__ __forceinline__ void face_core2(f2 ah, f2 wa, f2 bh, f2 bz, f2 wb, f2 Lh, f2 Lz,
-                                           f2 Lqn, f2 Lqt, f2 Rh, f2 Rz, f2 Rqn, f2 Rqt,
-                                           f2 &fh, f2 &fn, f2 &ft, f2 &sa, f2 &sb) {
+// Two faces in the face frame.  Inputs with beds measured from the minus
+// cell's bed: the edge states L (minus side) and R (plus side) -- depth, bed,
+// normal and tangential discharge -- the two cells' depths ah, bh and the
+// plus cell's bed bz.  Velocities are taken from the edge states, then the
+// hydrostatic step (HC/flucCal_2ndOrder_jh_improved_Kernel.cu:43-72), the HLLC
+// flux (:109-195, with the single-precision shortcuts of hllc<float, true>)
+// and the two bed-slope terms (:494-501).  fn / ft: normal / tangential
+// momentum flux; ft is linear in the tangential discharge, so a caller that
+// passes +q instead of -q for it takes -ft.
+//
+// The hydrostatic step runs with beds measured from the higher of the two edge
+// beds, o = max(Lz, Rz) (every operation of the scheme is invariant under a
+// common shift of z).  The upper edge then has bed 0 and its free surface is
+// its depth exactly, so a film of a few h_small on a bump keeps its depth to
+// the last bit instead of being rounded at the scale of the bed step (6e-8 m
+// per 0.5 m of relief in FP32), which decided which side of h_small such a
+// cell fell on.
+__device__ __forceinline__ void face_core2(f2 ah, f2 bh, f2 bz, f2 Lh, f2 Lz0, f2 Lqn, f2 Lqt,
+                                           f2 Rh, f2 Rz0, f2 Rqn, f2 Rqt, f2 &fh, f2 &fn,
+                                           f2 &ft, f2 &sa, f2 &sb) {
+  const f2 o = pk(fmaxf(Lz0.x, Rz0.x), fmaxf(Lz0.y, Rz0.y));
+  const f2 Lz = sub2(Lz0, o), Rz = sub2(Rz0, o);   // one of the two is exactly 0
+  const f2 bzo = sub2(bz, o);                       // the plus cell's bed
+  const f2 wa = sub2(ah, o), wb = add2(bzo, bh);    // the cells' free surfaces
   // velocities of the edge states
   const f2 il = pk(Lh.x < kHsF ? 0.f : rcpa(Lh.x), Lh.y < kHsF ? 0.f : rcpa(Lh.y));
   const f2 ir = pk(Rh.x < kHsF ? 0.f : rcpa(Rh.x), Rh.y < kHsF ? 0.f : rcpa(Rh.y));
@@ -171,8 +182,8 @@ __device__ __forceinline__ void face_core2(f2 ah, f2 wa, f2 bh, f2 bz, f2 wb, f2
   const f2 hR = pk(fmaxf(Rd.x, 0.f), fmaxf(Rd.y, 0.f));
   const f2 zL = sub2(Lw, hL), zR = sub2(Rw, hR);
   // bed-slope terms of both sides
-  sa = mul2(mul2(dup(kHalfGF), add2(ah, hL)), zL);
-  sb = mul2(mul2(dup(kHalfGF), add2(bh, hR)), sub2(zR, bz));
+  sa = mul2(mul2(dup(kHalfGF), add2(ah, hL)), add2(zL, o));  // zL - (the minus cell's bed, -o)
+  sb = mul2(mul2(dup(kHalfGF), add2(bh, hR)), sub2(zR, bzo));
   // HLLC
   const f2 qnL = mul2(uL, hL), qtL = mul2(vL, hL);
   const f2 qnR = mul2(uR, hR), qtR = mul2(vR, hR);
@@ -234,7 +245,6 @@ __device__ __forceinline__ Fc2 face2(const Cel2 &A, const Cel2 &B, const Slp2 &s
     return o;
   }
   const f2 bz = sub2(B.z, A.z);
-  const f2 wb = add2(bz, B.h);
   const f2 Lh = fma2(dup(0.5f), sA.h, A.h), Lz = mul2(dup(0.5f), sA.z);
   f2 Lqx = fma2(dup(0.5f), sA.qx, A.qx), Lqy = fma2(dup(0.5f), sA.qy, A.qy);
   const f2 Rh = fma2(dup(-0.5f), sB.h, B.h), Rz = fma2(dup(-0.5f), sB.z, bz);
@@ -246,13 +256,13 @@ __device__ __forceinline__ Fc2 face2(const Cel2 &A, const Cel2 &B, const Slp2 &s
   if (B.h.y < kHsF) Rqx.y = Rqy.y = 0.f;
   f2 fn, ft;
   if constexpr (DIR == 0) {
-    face_core2(A.h, A.h, B.h, bz, wb, Lh, Lz, Lqx, Lqy, Rh, Rz, Rqx, Rqy, o.fh, fn, ft, o.sa, o.sb);
+    face_core2(A.h, B.h, bz, Lh, Lz, Lqx, Lqy, Rh, Rz, Rqx, Rqy, o.fh, fn, ft, o.sa, o.sb);
     o.fx = fn;
     o.fy = ft;
   } else {
     // normal +y, tangent -x: the tangential discharge is passed as +qx, so
     // the face's x-momentum flux (-ft of the -qx form) is ft
-    face_core2(A.h, A.h, B.h, bz, wb, Lh, Lz, Lqy, Lqx, Rh, Rz, Rqy, Rqx, o.fh, fn, ft, o.sa, o.sb);
+    face_core2(A.h, B.h, bz, Lh, Lz, Lqy, Lqx, Rh, Rz, Rqy, Rqx, o.fh, fn, ft, o.sa, o.sb);
     o.fx = ft;
     o.fy = fn;
   }
@@ -298,8 +308,10 @@ __device__ __noinline__ Ghost1 ghost_face1(float ch, float cqx, float cqy, float
     cqn = -Cl.qy; cqt = Cl.qx; gqn = -G.qy; gqt = G.qx;
   }
   f2 fh, fn, ft, sa, sb;
-  face_core2(dup(Cl.h), dup(Cl.h), dup(G.h), dup(G.z), dup(G.wl), dup(Cl.h), dup(0.f), dup(cqn),
-             dup(cqt), dup(G.h), dup(G.z), dup(gqn), dup(gqt), fh, fn, ft, sa, sb);
+  // (every ghost has G.wl = G.z + G.h in C's frame, the free surface the
+  // face core forms from the bed and the depth)
+  face_core2(dup(Cl.h), dup(G.h), dup(G.z), dup(Cl.h), dup(0.f), dup(cqn), dup(cqt), dup(G.h),
+             dup(G.z), dup(gqn), dup(gqt), fh, fn, ft, sa, sb);
   r.sc = sa.x;
   if (side == 0) {  // C is the west side
     r.fh = fh.x; r.fx = fn.x; r.fy = ft.x;
