@@ -503,33 +503,99 @@ def first_order_rates(d: dict, dev, args, flush: torch.Tensor, stream, steps: in
     return out
 
 
-def ensemble_rate(dev, steps: int, count: int = 64, seed: int = 0) -> dict:
+def ensemble_rate(dev, steps: int, count: int = 64, seed: int = 0, plain_sample: int = 8) -> dict:
     """Config 3: `count` catchments (sides 256-1536, own hyetographs) advanced
-    together, one fused launch per step for all of them."""
+    together.  `value`: one persistent cooperative launch of `steps` steps for
+    all of them (hb_fused_run), replayed from a CUDA graph.  Beside it: the
+    same batch as one graph of `steps` per-step launch pairs, the autotuned
+    launch shape, 64 sequential single-instance fused runs, and the plain FP64
+    path (the reference's solver class on its own kernels) on a sample of the
+    catchments run one after another."""
     from hipims_b200 import autotune, scenarios as S
     from hipims_b200.fused import FusedSolver
     from hipims_b200.scenarios import catchment_from
 
-    cs = [catchment_from(d) for d in S.ensemble(count, seed=seed)]
+    ds = S.ensemble(count, seed=seed)
+    cs = [catchment_from(d) for d in ds]
     cfg = autotune.tune(cs, torch.float32, dev, steps=4)
+    st = torch.cuda.current_stream(dev)
+
+    def timed(fn) -> float:
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        a.record(st)
+        fn()
+        b.record(st)
+        torch.cuda.synchronize(dev)
+        return a.elapsed_time(b)
+
+    # persistent: one launch of `steps` steps, replayed from a graph
+    fp = FusedSolver(cs, dtype=torch.float32, device=dev, tile=(32, 64),
+                     minb=cfg.get("minb", 0) if tuple(cfg["tile"]) == (32, 64) else 0)
+    cells = sum(i.n_valid for i in fp.inst)
+    fp.step(SPINUP)
+    fp.capture_persistent(steps)
+    fp.replay()  # warm-up replay
+    ms_p = timed(fp.replay)
+    fp.check()
+    del fp
+    torch.cuda.empty_cache()
+    # per-step launch pairs, autotuned shape, replayed from a graph
     fs = FusedSolver(cs, dtype=torch.float32, device=dev, tile=cfg["tile"],
                      minb=cfg.get("minb", 0))
-    cells = sum(i.n_valid for i in fs.inst)
     fs.step(SPINUP)
     fs.capture(steps)
-    fs.replay()  # warm-up replay
-    st = torch.cuda.current_stream(dev)
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize(dev)
-    a.record(st)
     fs.replay()
-    b.record(st)
-    torch.cuda.synchronize(dev)
-    ms = a.elapsed_time(b)
-    return {"value": cells * steps / (ms * 1e-3) / 1e9, "unit": METRIC, "instances": count,
-            "cells": cells, "steps": steps, "ms_per_step": ms / steps,
-            "launch": "one CUDA-graph replay of `steps` fused launches for all instances",
-            "tile": list(cfg["tile"]), "minb": cfg.get("minb", 0)}
+    ms_s = timed(fs.replay)
+    del fs
+    torch.cuda.empty_cache()
+    # 64 sequential single-instance runs, each `steps` launches after spin-up
+    ms_seq = 0.0
+    for c in cs:
+        f1 = FusedSolver(c, dtype=torch.float32, device=dev, tile=(32, 64))
+        f1.step(SPINUP)
+        ms_seq += timed(lambda: f1.step(steps))
+        del f1
+    torch.cuda.empty_cache()
+    # the plain FP64 path on every (count // plain_sample)-th catchment, one after another
+    plain = None
+    picked = ds[:: max(count // plain_sample, 1)][:plain_sample]
+    pl_cells, pl_s = 0, 0.0
+    for d in picked:
+        r = plain_fp64_rate(d, dev, steps=5, reference_kernels=True)
+        if not r.get("value"):
+            plain = r
+            break
+        n = int(np.sum(np.asarray(d["mask"]) > 0))
+        pl_cells += n * 5
+        pl_s += n * 5 / (r["value"] * 1e9)
+    if plain is None and pl_s > 0:
+        plain = {"value": pl_cells / pl_s / 1e9, "unit": METRIC, "catchments": len(picked),
+                 "steps_each": 5, "path": r["path"] + ", catchments one after another"}
+    value = cells * steps / (ms_p * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+    achieved = BYTES_PER_CELL_FP32 * cells * steps / (ms_p * 1e-3) / 1e9
+    out = {"value": value, "unit": METRIC, "instances": count, "cells": cells, "steps": steps,
+           "ms_per_step": ms_p / steps,
+           "launch": f"one persistent cooperative launch (hb_fused_run) of {steps} steps for all "
+                     f"instances, replayed from a CUDA graph",
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "peak_source": peak_kind},
+           "per_step_launches": {"value": cells * steps / (ms_s * 1e-3) / 1e9, "unit": METRIC,
+                                 "tile": list(cfg["tile"]), "minb": cfg.get("minb", 0),
+                                 "cells_per_lane": autotune.cells_per_lane(cfg),
+                                 "launch": f"one CUDA-graph replay of {steps} per-step launch "
+                                           f"pairs (autotuned shape)"},
+           "sequential_single_runs": {"value": cells * steps / (ms_seq * 1e-3) / 1e9,
+                                      "unit": METRIC,
+                                      "path": f"{count} single-instance fused FP32 runs, one "
+                                              f"after another, {steps} steps each"}}
+    out["over_sequential_single_runs"] = value / out["sequential_single_runs"]["value"]
+    if plain is not None:
+        out["sequential_plain_fp64"] = plain
+        if plain.get("value"):
+            out["over_sequential_plain_fp64"] = value / plain["value"]
+    return out
 
 
 def adjoint_cost(dev, n: int = 1024, steps: int = 2000, K: int = 100, every: int = 10,

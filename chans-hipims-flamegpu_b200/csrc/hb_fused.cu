@@ -2072,9 +2072,14 @@ int encode_maps(const hb_fused_batch *b, cudaStream_t st, CUtensorMap *host_maps
 
 using namespace hb;
 
+// the persistent step's counters (3 x uint64), after the tensor maps
+inline size_t ws_sync_offset(const hb_fused_batch *b) {
+  return align256(ws_maps_offset(b) + (size_t)b->n_instances * kMapsPerInstance * sizeof(CUtensorMap));
+}
+
 extern "C" size_t hb_fused_workspace_size(const hb_fused_batch *b) {
   if (!b) return 0;
-  return ws_maps_offset(b) + (size_t)b->n_instances * kMapsPerInstance * sizeof(CUtensorMap);
+  return ws_sync_offset(b) + 256;
 }
 
 namespace hb {
@@ -2358,4 +2363,70 @@ extern "C" int hb_fused_step_noalloc(const hb_fused_batch *b, int nsteps, int pr
   }
   local.workspace = g_noalloc_ptr[dev];
   return hb_fused_step(&local, nsteps, stream);
+}
+
+// ---------------------------------------------------------------------------
+// hb_fused_run: nsteps steps of every instance in one persistent cooperative
+// launch (FP32 2nd order, 32 x 64 tiles).
+// ---------------------------------------------------------------------------
+namespace hb {
+namespace {
+
+template <bool SOURCES>
+int launch_persistent(const hb_fused_batch *b, int nsteps, long long budget, cudaStream_t st) {
+  using S = PairSmem<32>;
+  auto *kern = pairs_persistent_kernel<32, SOURCES>;
+  int rc = set_smem_attr(reinterpret_cast<const void *>(kern), (int)sizeof(S));
+  if (rc) return rc;
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kRowsNT, sizeof(S));
+  if (e != cudaSuccess || per_sm < 1)
+    return set_error(HB_ERR_CUDA, "hb_fused_run: occupancy: %s",
+                     e != cudaSuccess ? cudaGetErrorString(e) : "no resident block");
+  int grid = per_sm * num_sms();
+  if (grid > b->n_tiles) grid = b->n_tiles;
+  char *ws = reinterpret_cast<char *>(b->workspace);
+  const hb_instance *insts = b->instances;
+  const int32_t *tile_inst = b->tile_instance;
+  const int32_t *order = reinterpret_cast<const int32_t *>(ws + ws_order_offset(b));
+  const int32_t *counts = reinterpret_cast<const int32_t *>(ws + ws_counts_offset(b));
+  const uint8_t *allvalid = reinterpret_cast<const uint8_t *>(ws + ws_flags_offset(b));
+  TilePartial *parts = reinterpret_cast<TilePartial *>(ws);
+  TilePartial *gparts = reinterpret_cast<TilePartial *>(ws + ws_partials_bytes(b->n_tiles));
+  unsigned *gcount = reinterpret_cast<unsigned *>(ws + ws_gcount_offset(b));
+  BcTable *bct = reinterpret_cast<BcTable *>(ws + ws_bct_offset(b));
+  const CUtensorMap *maps = reinterpret_cast<const CUtensorMap *>(ws + ws_maps_offset(b));
+  unsigned long long *sync = reinterpret_cast<unsigned long long *>(ws + ws_sync_offset(b));
+  int n_instances = b->n_instances;
+  e = cudaMemsetAsync(sync, 0, 3 * sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return set_error(HB_ERR_CUDA, "hb_fused_run: %s", cudaGetErrorString(e));
+  void *args[] = {(void *)&insts, (void *)&tile_inst, (void *)&order, (void *)&counts,
+                  (void *)&allvalid, (void *)&parts, (void *)&gparts, (void *)&gcount,
+                  (void *)&bct, (void *)&maps, (void *)&n_instances, (void *)&nsteps,
+                  (void *)&sync, (void *)&budget};
+  e = cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(kern), dim3(grid), dim3(kRowsNT),
+                                  args, sizeof(S), st);
+  if (e != cudaSuccess)
+    return set_error(HB_ERR_CUDA, "hb_fused_run: cooperative launch of %d blocks: %s", grid,
+                     cudaGetErrorString(e));
+  return HB_OK;
+}
+
+}  // namespace
+}  // namespace hb
+
+extern "C" int hb_fused_run(const hb_fused_batch *b, int nsteps, long long budget_cycles,
+                            void *stream) {
+  if (!b || !b->instances || !b->tile_instance || !b->workspace || b->n_tiles <= 0)
+    return set_error(HB_ERR_ARG, "hb_fused_run: bad batch record");
+  if (nsteps < 0) return set_error(HB_ERR_ARG, "hb_fused_run: negative nsteps");
+  if (!uses_rows_kernel(b) || b->tile_x != kPW || b->tile_y != 32 || b->dtype != HB_F32 ||
+      b->order != 2 || (b->flags & HB_FLAG_EXACT_FP32))
+    return set_error(HB_ERR_ARG, "hb_fused_run: the persistent step is built for the FP32 "
+                                 "2nd-order step with 32 x 64 tiles");
+  if (nsteps == 0) return HB_OK;
+  const long long budget = budget_cycles > 0 ? budget_cycles : (1LL << 31);
+  auto st = as_stream(stream);
+  if (b->flags & HB_FLAG_SOURCES) return launch_persistent<true>(b, nsteps, budget, st);
+  return launch_persistent<false>(b, nsteps, budget, st);
 }

@@ -470,9 +470,489 @@ __device__ __forceinline__ Fc2 face_pair(const PairSmem<TY> &s, const Cel2 &A, c
 }
 
 // ===========================================================================
-// The step kernel (FP32, 2nd order).  PATH 0: general tiles (no-data cells,
-// ghost faces or the cell-0 rule's cell in reach); PATH 1: all-valid tiles.
+// One tile of a step (FP32, 2nd order): stage it, evaluate its faces, update
+// its cells, write its partial sums, and close its group / finalize its
+// instance when it is the last.  PATH 0: a general tile (no-data cells, ghost
+// faces or the cell-0 rule's cell in reach); PATH 1: an all-valid tile.
+// Returns false when the tile's data did not arrive within the bounded wait
+// (the instance's status says so; the caller leaves).
 // ===========================================================================
+template <int TY, bool SOURCES, int PATH>
+__device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, const int tile,
+                                          const hb_instance *__restrict__ insts,
+                                          const int32_t *__restrict__ tile_inst,
+                                          TilePartial *__restrict__ partials,
+                                          TilePartial *__restrict__ gparts,
+                                          unsigned *__restrict__ gcount, BcTable *__restrict__ bct,
+                                          const CUtensorMap *__restrict__ maps) {
+  constexpr bool kAllValid = PATH == 1;
+  constexpr bool ALLV = kAllValid;
+  using S = PairSmem<TY>;
+  constexpr int R = S::R;
+  const PairView<TY> V{s};
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int ii = tile_inst[tile];
+  const hb_instance &in = insts[ii];
+  hb_ctrl *ctrl = in.ctrl;
+  if (__ldcg(&ctrl->halted)) return true;
+  const int lt = tile - in.tile_begin;
+  const int tyi = lt / in.tiles_x, txi = lt - tyi * in.tiles_x;
+  const int y0 = tyi * TY, x0 = txi * kPW;
+  // the control block changes between steps (a persistent launch reads it
+  // again after every grid barrier): loads that bypass L1
+  const int cur = __ldcg(&ctrl->cur);
+  const double t = __ldcg(&ctrl->t);
+  const float dt = (float)__ldcg(&ctrl->dt);
+  const float dx = (float)in.dx;
+  const float rain = (float)__ldcg(&ctrl->rain_rate);
+  const bool first = (t == 0.0);
+  const int P = in.pitch;
+  const CUtensorMap *m = maps + (size_t)ii * kMapsPerInstance;
+
+  if (tid == 0) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&s.bar, S::kTxBytes);
+    tma_load_2d(s.f[0], m + 0 + cur, x0, y0, &s.bar);
+    tma_load_2d(s.f[1], m + 2 + cur, x0, y0, &s.bar);
+    tma_load_2d(s.f[2], m + 4 + cur, x0, y0, &s.bar);
+    tma_load_2d(s.f[3], m + 6, x0, y0, &s.bar);
+    tma_load_2d(s.hmax, m + 7, x0 + HB_PAD_X, y0 + HB_PAD_Y, &s.bar);
+    tma_load_2d(s.code, m + 8, x0, y0, &s.bar);
+  }
+  if (tid < HB_MAX_CLASSES) {
+    if constexpr (!kAllValid) {
+      s.bctype[tid] = in.bc_type[tid];
+      for (int q = 0; q < 4; q++) s.bc[tid][q] = __ldcg(&bct[ii].v[tid][q]);
+    }
+  } else if (tid >= 64 && tid < 64 + HB_MAX_ZONES) {
+    s.manning[tid - 64] = (float)in.manning[tid - 64];
+  }
+  const int bug_y = in.bug_y, bug_x = in.bug_x;
+  float datum_tile = 0.f;
+  if (in.datum) {
+    const int by = y0 / HB_DATUM_BLOCK, bx = x0 / HB_DATUM_BLOCK;
+    datum_tile = in.datum[by * in.datum_nx + bx];
+    if (tid >= 32 && tid < 41) {
+      const int q = tid - 32, dyb = q / 3 - 1, dxb = q % 3 - 1;
+      const int yy = min(max(by + dyb, 0), in.datum_ny - 1);
+      const int xx = min(max(bx + dxb, 0), in.datum_nx - 1);
+      s.ddatum[q] = in.datum[yy * in.datum_nx + xx] - datum_tile;
+    }
+  }
+  const bool arrived = mbar_wait(&s.bar, phase, 4000000000LL);
+  if (__syncthreads_or(!arrived)) {
+    if (tid == 0) atomicOr(&ctrl->status, 2);
+    mbar_wait(&s.bar, phase, 4000000000LL);
+    return false;
+  }
+  phase ^= 1u;
+  if (in.datum) {
+    __syncthreads();  // ddatum visible
+    const int by0 = (y0 / HB_DATUM_BLOCK) * HB_DATUM_BLOCK;
+    const int bx0 = (x0 / HB_DATUM_BLOCK) * HB_DATUM_BLOCK;
+    const DatumHalo dh = datum_halo(y0, x0, by0, bx0, TY, kPW, kPSWF, HB_DATUM_BLOCK);
+    const int NH = dh.count();
+    for (int q = tid; q < NH; q += kRowsNT) {
+      int i, j;
+      datum_halo_cell(dh, q, TY, kPW, kPSWF, i, j);
+      const int ry = y0 + i, rx = x0 + j;
+      const int dyb = ry < by0 ? 0 : (ry >= by0 + HB_DATUM_BLOCK ? 2 : 1);
+      const int dxb = rx < bx0 ? 0 : (rx >= bx0 + HB_DATUM_BLOCK ? 2 : 1);
+      if (dyb != 1 || dxb != 1) s.f[3][V.fi(i, j)] += s.ddatum[dyb * 3 + dxb];
+    }
+  }
+  __syncthreads();
+
+  // --- tile edges: warp 0 the faces between columns 63 | 64 (east faces of
+  // lane 31's second cell), two rows per lane; warp 1 the x-slopes of
+  // column -1 (west neighbour of lane 0's first cell)
+  if (w == 0) {
+    for (int i = 2 * lane; i < TY; i += 64) {
+      float a[4], b[4];  // slopes of col 63 / col 64 for rows i, i + 1 (h, z, qx, qy)
+      float a1[4], b1[4];
+      xslope1<TY, ALLV>(V, i, 63, a[0], a[1], a[2], a[3]);
+      xslope1<TY, ALLV>(V, i + 1, 63, a1[0], a1[1], a1[2], a1[3]);
+      xslope1<TY, ALLV>(V, i, 64, b[0], b[1], b[2], b[3]);
+      xslope1<TY, ALLV>(V, i + 1, 64, b1[0], b1[1], b1[2], b1[3]);
+      const Slp2 sA{pk(a[0], a1[0]), pk(a[1], a1[1]), pk(a[2], a1[2]), pk(a[3], a1[3])};
+      const Slp2 sB{pk(b[0], b1[0]), pk(b[1], b1[1]), pk(b[2], b1[2]), pk(b[3], b1[3])};
+      const Fc2 f = face_pair<0, ALLV>(s, V.vpair(i, 63), V.vpair(i, 64), sA, sB,
+                                       V.code(i, 63), V.code(i + 1, 63), V.code(i, 64),
+                                       V.code(i + 1, 64), datum_tile);
+      s.xe[i][0] = f.fh.x; s.xe[i][1] = f.fx.x; s.xe[i][2] = f.fy.x; s.xe[i][3] = f.sa.x;
+      s.xe[i + 1][0] = f.fh.y; s.xe[i + 1][1] = f.fx.y; s.xe[i + 1][2] = f.fy.y;
+      s.xe[i + 1][3] = f.sa.y;
+    }
+  } else if (w == 1) {
+    for (int i = lane; i < TY; i += 32) {
+      float sh, sz, sqx, sqy;
+      xslope1<TY, ALLV>(V, i, -1, sh, sz, sqx, sqy);
+      s.sxw[i][0] = sh;
+      s.sxw[i][1] = sz;
+      s.sxw[i][2] = sqx;
+      s.sxw[i][3] = sqy;
+    }
+  }
+
+  const int r0 = w * R;
+  const int j0 = 2 * lane;  // this lane's first column
+  const int rx0 = x0 + j0;
+  f2 vol2 = dup(0.f);
+  float smax_t = 0.f;
+  double outf = 0.0;
+  int any_dry = 0;
+  {
+    // validity of a pair as two floats (1 valid, 0 not); all-valid: 1
+    auto vpair = [&](int i) -> f2 {
+      if constexpr (ALLV) {
+        (void)i;
+        return dup(1.f);
+      } else {
+        return pk(is_valid(V.code(i, j0)) ? 1.f : 0.f, is_valid(V.code(i, j0 + 1)) ? 1.f : 0.f);
+      }
+    };
+    // --- column window of the pair: row r0 and its y-slopes, the face
+    // between rows r0-1 and r0, the depths of row r0-1
+    Cel2 C = V.pair(r0, j0);
+    f2 vC = vpair(r0), vN = vpair(r0 - 1);
+    f2 Nh;
+    Slp2 syC;
+    Fc2 nf;
+    {
+      const Cel2 N = V.pair(r0 - 1, j0), NN = V.pair(r0 - 2, j0), S1 = V.pair(r0 + 1, j0);
+      const Slp2 syN = yslope2<ALLV>(N, C, vC, NN, vpair(r0 - 2));
+      syC = yslope2<ALLV>(C, S1, vpair(r0 + 1), N, vN);
+      // face between rows r0-1 (north, B) and r0 (south, A)
+      nf = face_pair<1, ALLV>(s, C, N, syC, syN, V.code(r0, j0), V.code(r0, j0 + 1),
+                              V.code(r0 - 1, j0), V.code(r0 - 1, j0 + 1), datum_tile);
+      Nh = N.h;
+    }
+    __syncthreads();  // tile-edge faces and slopes ready
+    float *hout = (float *)in.h[1 - cur];
+    float *qxout = (float *)in.qx[1 - cur];
+    float *qyout = (float *)in.qy[1 - cur];
+    float *hmaxg = (float *)in.h_max;
+    const bool infil = SOURCES && in.cum != nullptr;
+    const bool stations = SOURCES && in.rain_station != nullptr;
+    const bool fwd_tile = (y0 < HB_PAD_Y && in.halo_up[0] != nullptr) ||
+                          (y0 + TY > in.rows - HB_PAD_Y && in.halo_down[0] != nullptr);
+    const f2 r2 = dup(dt / dx);
+    const float rdt = rain * dt;
+    const float dtg = dt * kGF;
+
+#pragma unroll 1
+    for (int i = r0; i < r0 + R; ++i) {
+      // --- x-direction: neighbours W (col 2j-1) and E (col 2j+2)
+      const int kc = V.fi(i, j0);
+      float Wv[4], Ev[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        Wv[q] = s.f[q][kc - 1];
+        Ev[q] = s.f[q][kc + 2];
+      }
+      uint8_t kW = 0, kE = 0;
+      const uint8_t kA = V.code(i, j0), kB = V.code(i, j0 + 1);
+      bool vWb = true, vAb = true, vBb = true, vEb = true;
+      if constexpr (!ALLV) {
+        kW = V.code(i, j0 - 1);
+        kE = V.code(i, j0 + 2);
+        vWb = is_valid(kW);
+        vAb = is_valid(kA);
+        vBb = is_valid(kB);
+        vEb = is_valid(kE);
+      }
+      // x-slopes of cells a = 2j and b = 2j+1 (fields h, qx, qy, z)
+      const float cA[4] = {C.h.x, C.qx.x, C.qy.x, C.z.x};
+      const float cB[4] = {C.h.y, C.qx.y, C.qy.y, C.z.y};
+      float sxa[4], sxb[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        sxa[q] = slope1(cA[q], vWb ? Wv[q] : cA[q], vBb ? cB[q] : cA[q]);
+        sxb[q] = slope1(cB[q], vAb ? cA[q] : cB[q], vEb ? Ev[q] : cB[q]);
+      }
+      // slope of col 2j-1 from the west lane (lane 0: the pre-pass)
+      float sw[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) sw[q] = __shfl_up_sync(0xffffffffu, sxb[q], 1);
+      if (lane == 0) {
+        sw[0] = s.sxw[i][0];
+        sw[3] = s.sxw[i][1];
+        sw[1] = s.sxw[i][2];
+        sw[2] = s.sxw[i][3];
+      }
+      // --- west faces of a and b: (2j-1 | 2j) and (2j | 2j+1)
+      f2 Px_h, Px_x, Px_y;  // x-direction flux differences (west - east) of the pair
+      f2 wfh;               // west-face mass flux (outflow of boundary faces)
+      f2 efh;               // east-face mass flux
+      {
+        const Cel2 Aw{pk(Wv[0], C.h.x), pk(Wv[1], C.qx.x), pk(Wv[2], C.qy.x), pk(Wv[3], C.z.x)};
+        const Slp2 sAw{pk(sw[0], sxa[0]), pk(sw[3], sxa[3]), pk(sw[1], sxa[1]), pk(sw[2], sxa[2])};
+        const Slp2 sBw{pk(sxa[0], sxb[0]), pk(sxa[3], sxb[3]), pk(sxa[1], sxb[1]), pk(sxa[2], sxb[2])};
+        const Fc2 wf = face_pair<0, ALLV>(s, Aw, C, sAw, sBw, kW, kA, kA, kB, datum_tile);
+        // east faces: a's is the lane's second west face; b's comes from lane j+1
+        float e_h = __shfl_down_sync(0xffffffffu, wf.fh.x, 1);
+        float e_x = __shfl_down_sync(0xffffffffu, wf.fx.x, 1);
+        float e_y = __shfl_down_sync(0xffffffffu, wf.fy.x, 1);
+        float e_a = __shfl_down_sync(0xffffffffu, wf.sa.x, 1);
+        if (lane == 31) {
+          e_h = s.xe[i][0];
+          e_x = s.xe[i][1];
+          e_y = s.xe[i][2];
+          e_a = s.xe[i][3];
+        }
+        const f2 ef_h = pk(wf.fh.y, e_h), ef_x = pk(wf.fx.y, e_x), ef_y = pk(wf.fy.y, e_y),
+                 ef_a = pk(wf.sa.y, e_a);
+        Px_h = sub2(wf.fh, ef_h);
+        Px_x = add2(sub2(sub2(wf.fx, ef_x), ef_a), wf.sb);
+        Px_y = sub2(wf.fy, ef_y);
+        wfh = wf.fh;
+        efh = ef_h;
+      }
+      // --- the row below, its y-slopes, and the south faces: rows i+1 (A) | i (B)
+      const Cel2 Sx = V.pair(i + 1, j0);
+      const f2 vS = vpair(i + 1);
+      Fc2 sf;
+      Slp2 syS;
+      {
+        const Cel2 SS = V.pair(i + 2, j0);
+        syS = yslope2<ALLV>(Sx, SS, vpair(i + 2), C, vC);
+        uint8_t kSa = 0, kSb = 0;
+        if constexpr (!ALLV) {
+          kSa = V.code(i + 1, j0);
+          kSb = V.code(i + 1, j0 + 1);
+        }
+        sf = face_pair<1, ALLV>(s, Sx, C, syS, syC, kSa, kSb, kA, kB, datum_tile);
+      }
+
+      // --- cell updates
+      const int ry = y0 + i;
+      // fluxMask activity (HC/fluxMaskGenerator_Kernel.cu:19-42)
+      bool act0 = first || C.h.x > kHsF, act1 = first || C.h.y > kHsF;
+      if (!(act0 && act1)) {
+        if constexpr (ALLV) {
+          act0 = act0 || C.h.y > kHsF || Nh.x > kHsF || Wv[0] > kHsF || Sx.h.x > kHsF;
+          act1 = act1 || Ev[0] > kHsF || Nh.y > kHsF || C.h.x > kHsF || Sx.h.y > kHsF;
+        } else {
+          const int ra = rx0, rb = rx0 + 1;
+          auto nb = [&](bool v, int yy, int xx, float hh) {
+            return v && !(yy == bug_y && xx == bug_x) && hh > kHsF;
+          };
+          act0 = act0 || nb(vBb, ry, ra + 1, C.h.y) || nb(vN.x != 0.f, ry - 1, ra, Nh.x) ||
+                 nb(vWb, ry, ra - 1, Wv[0]) || nb(vS.x != 0.f, ry + 1, ra, Sx.h.x);
+          act1 = act1 || nb(vEb, ry, rb + 1, Ev[0]) || nb(vN.y != 0.f, ry - 1, rb, Nh.y) ||
+                 nb(vAb, ry, rb - 1, C.h.x) || nb(vS.y != 0.f, ry + 1, rb, Sx.h.y);
+        }
+      }
+      f2 hu = mul2(add2(Px_h, sub2(sf.fh, nf.fh)), r2);
+      f2 qxu = mul2(add2(Px_x, sub2(sf.fx, nf.fx)), r2);
+      f2 qyu = mul2(add2(Px_y, add2(sub2(sub2(sf.fy, nf.fy), nf.sa), sf.sb)), r2);
+      if (!act0) hu.x = qxu.x = qyu.x = 0.f;
+      if (!act1) hu.y = qxu.y = qyu.y = 0.f;
+      if constexpr (!ALLV) {
+        // outflow through boundary faces of active valid cells
+        const bool bE0 = !vBb, bW0 = !vWb, bN0 = vN.x == 0.f, bS0 = vS.x == 0.f;
+        const bool bE1 = !vEb, bW1 = !vAb, bN1 = vN.y == 0.f, bS1 = vS.y == 0.f;
+        if (vAb && act0 && (bE0 | bW0 | bN0 | bS0)) {
+          double o = 0.0;
+          if (bE0) o += (double)efh.x;
+          if (bN0) o += (double)nf.fh.x;
+          if (bW0) o -= (double)wfh.x;
+          if (bS0) o -= (double)sf.fh.x;
+          outf += o;
+        }
+        if (vBb && act1 && (bE1 | bW1 | bN1 | bS1)) {
+          double o = 0.0;
+          if (bE1) o += (double)efh.y;
+          if (bN1) o += (double)nf.fh.y;
+          if (bW1) o -= (double)wfh.y;
+          if (bS1) o -= (double)sf.fh.y;
+          outf += o;
+        }
+      }
+      // rain (HP/SWE_CUDA.py:549 / HC/stationPrecipitation_Kernel.cu:27)
+      const size_t go = (size_t)(ry + HB_PAD_Y) * P + (rx0 + HB_PAD_X);
+      if (stations) {
+        hu.x += (float)__ldcg(&in.station_rate[in.rain_station[go]]) * dt;
+        hu.y += (float)__ldcg(&in.station_rate[in.rain_station[go + 1]]) * dt;
+      } else {
+        hu = add2(hu, dup(rdt));
+      }
+      if (infil) {
+        // Green-Ampt infiltration on the active cells, after rain
+        // (HC/infiltrationCUDA_Kernel.cu:20-46; order HP/CatchFlood_main.py:164-170)
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+          const bool act = c ? act1 : act0;
+          const bool vc = c ? vBb : vAb;
+          if (!(act && vc)) continue;
+          const uint8_t kc_ = c ? kB : kA;
+          const float hc = c ? C.h.y : C.h.x;
+          float *cum = (float *)in.cum + go + c;
+          const int zc = kc_ & 15;
+          const float K = (float)in.ks[zc], psi = (float)in.psi[zc], dth = (float)in.dtheta[zc];
+          const float F0 = *cum;
+          const float a = F0 + dt * K;
+          const float F1 = 0.5f * (a + sqrtf(a * a + 4.f * dt * K * (psi + hc) * dth));
+          const float dF = fminf(hc, F1 - F0);
+          *cum = F0 + dF;
+          if (c) hu.y -= dF; else hu.x -= dF;
+        }
+      }
+      // implicit friction + update (HC/friction_implicit_andUpdate_jh_Kernel.cu:22-146)
+      const f2 h2 = add2(C.h, hu);
+      f2 qx2 = add2(C.qx, qxu), qy2 = add2(C.qy, qyu);
+      f2 sgh = dup(0.f), ih = dup(0.f);
+      const f2 nman = pk(s.manning[kA & 15], s.manning[kB & 15]);
+      {
+        const f2 gh = mul2(dup(kGF), h2);
+        sgh = pk(sqrta(gh.x), sqrta(gh.y));
+        ih = pk(rcpa(h2.x), rcpa(h2.y));
+        const f2 qq = fma2(qx2, qx2, mul2(qy2, qy2));
+        const f2 qn = pk(sqrta(qq.x), sqrta(qq.y));
+        const f2 cb = pk(ex2a(lg2a(h2.x) * (-1.f / 3.f)), ex2a(lg2a(h2.y) * (-1.f / 3.f)));
+        const f2 a = mul2(mul2(mul2(mul2(mul2(dup(dtg), nman), nman), cb), ih), ih);
+        const f2 sq = fma2(mul2(dup(4.f), a), qn, dup(1.f));
+        const f2 den = add2(dup(1.f), pk(sqrta(sq.x), sqrta(sq.y)));
+        const f2 fct = pk(2.f * rcpa(den.x), 2.f * rcpa(den.y));
+        const f2 lim = mul2(mul2(dup(5.f), h2), sgh);
+        const f2 tx = mul2(qx2, fct), ty = mul2(qy2, fct);
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+          const float hh = c ? h2.y : h2.x;
+          float &qx = c ? qx2.y : qx2.x;
+          float &qy = c ? qy2.y : qy2.x;
+          if (hh < kHsF) {
+            qx = 0.f;
+            qy = 0.f;
+            if (c) { sgh.y = 0.f; ih.y = 0.f; } else { sgh.x = 0.f; ih.x = 0.f; }
+            continue;
+          }
+          if (!((c ? nman.y : nman.x) > 0.f)) continue;
+          const float l = c ? lim.y : lim.x;
+          if (fabsf(qx) > 1.0e-10f) {
+            const float temp = c ? tx.y : tx.x;
+            if (fabsf(temp) > l) {
+              const float q2 = 2.f * temp - qx;
+              qx = (q2 * temp <= 0.f) ? 0.f : q2;
+            } else {
+              qx = temp;
+            }
+          }
+          if (fabsf(qy) > 1.0e-10f) {
+            const float temp = c ? ty.y : ty.x;
+            if (fabsf(temp) > l) {
+              const float q2 = 2.f * temp - qy;
+              qy = (q2 * temp <= 0.f) ? 0.f : q2;
+            } else {
+              qy = temp;
+            }
+          }
+        }
+      }
+      // stores: both cells valid (every all-valid tile), else per cell
+      const f2 hm_old = *reinterpret_cast<const f2 *>(&s.hmax[i * kPW + j0]);
+      const f2 hm = pk(fmaxf(h2.x, hm_old.x), fmaxf(h2.y, hm_old.y));
+      if (vAb && vBb) {
+        *reinterpret_cast<f2 *>(hout + go) = h2;
+        *reinterpret_cast<f2 *>(qxout + go) = qx2;
+        *reinterpret_cast<f2 *>(qyout + go) = qy2;
+        *reinterpret_cast<f2 *>(hmaxg + go) = hm;
+      } else {
+        if (vAb) {
+          hout[go] = h2.x; qxout[go] = qx2.x; qyout[go] = qy2.x; hmaxg[go] = hm.x;
+        }
+        if (vBb) {
+          hout[go + 1] = h2.y; qxout[go + 1] = qx2.y; qyout[go + 1] = qy2.y; hmaxg[go + 1] = hm.y;
+        }
+      }
+      if (fwd_tile) {
+        const int ob = 1 - cur;
+        auto fwd = [&](void *const *dst, int row) {
+          const size_t gh = (size_t)row * P + (rx0 + HB_PAD_X);
+          if (vAb) {
+            ((float *)dst[ob])[gh] = h2.x;
+            ((float *)dst[2 + ob])[gh] = qx2.x;
+            ((float *)dst[4 + ob])[gh] = qy2.x;
+          }
+          if (vBb) {
+            ((float *)dst[ob])[gh + 1] = h2.y;
+            ((float *)dst[2 + ob])[gh + 1] = qx2.y;
+            ((float *)dst[4 + ob])[gh + 1] = qy2.y;
+          }
+        };
+        if (ry < HB_PAD_Y && in.halo_up[0] != nullptr)
+          fwd(in.halo_up, in.halo_up_rows + HB_PAD_Y + ry);
+        if (ry >= in.rows - HB_PAD_Y && in.halo_down[0] != nullptr)
+          fwd(in.halo_down, ry - in.rows + HB_PAD_Y);
+        // the neighbour may be a peer GPU: order these stores system-wide
+        // before this tile's partial, its group count and the host's next
+        // collective
+        __threadfence_system();
+      }
+      // CFL speed (HC/timeControl_Kernel.cu:186-189), volume
+      const f2 sp = fma2(pk(fmaxf(fabsf(qx2.x), fabsf(qy2.x)), fmaxf(fabsf(qx2.y), fabsf(qy2.y))),
+                         ih, sgh);
+      if (vAb) {
+        if (h2.x > kHsF) smax_t = fmaxf(smax_t, sp.x); else any_dry = 1;
+      }
+      if (vBb) {
+        if (h2.y > kHsF) smax_t = fmaxf(smax_t, sp.y); else any_dry = 1;
+      }
+      vol2 = add2(vol2, pk(vAb ? h2.x : 0.f, vBb ? h2.y : 0.f));
+
+      // slide the column window down one row
+      nf = sf;
+      Nh = C.h;
+      vN = vC;
+      C = Sx;
+      vC = vS;
+      syC = syS;
+    }
+  }
+
+  // --- tile partials and the instance's last-tile finalize
+  double vol = warp_sum((double)vol2.x + (double)vol2.y);
+  if constexpr (!kAllValid) outf = warp_sum(outf);
+  const double smax = (double)warp_max(smax_t);
+  any_dry = __any_sync(0xffffffffu, any_dry);
+  if (lane == 0) {
+    s.red_d[0][w] = vol;
+    s.red_d[1][w] = outf;
+    s.red_s[w] = smax;
+    s.red_i[w] = any_dry;
+  }
+  __syncthreads();
+  const int n_inst_tiles = in.tiles_x * in.tiles_y;
+  const int grp = lt / kGroupTiles;
+  const int gsize = min(kGroupTiles, n_inst_tiles - grp * kGroupTiles);
+  const int gbase = in.tile_begin / kGroupTiles + ii;
+  if (tid == 0) {
+    TilePartial p;
+    p.volume = p.outflow = p.smax = 0.0;
+    p.any_dry = 0;
+    p.pad = 0;
+    for (int q = 0; q < kRowsNW; q++) {
+      p.volume += s.red_d[0][q];
+      p.outflow += s.red_d[1][q];
+      p.smax = fmax(p.smax, s.red_s[q]);
+      p.any_dry |= s.red_i[q];
+    }
+    partials[tile] = p;
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> done(gcount[gbase + grp]);
+    s.last = (done.fetch_add(1u, cuda::memory_order_acq_rel) == (unsigned)(gsize - 1));
+  }
+  __syncthreads();
+  if (s.last)
+    close_group<float, kRowsNT>(in, ii, partials + in.tile_begin + grp * kGroupTiles, gsize,
+                                gparts, gcount, gbase + grp, gbase,
+                                (n_inst_tiles + kGroupTiles - 1) / kGroupTiles, bct, s.red_d,
+                                s.red_s, s.red_i, &s.last2);
+  __syncthreads();
+  return true;
+}
+
+// The step kernel: one launch per step and build, one CTA per tile by
+// default (a positive grid loops over the build's tiles).
 template <int TY, int MINB, bool SOURCES, int PATH>
 __global__ void __launch_bounds__(kRowsNT, MINB)
 pairs_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restrict__ tile_inst,
@@ -480,479 +960,132 @@ pairs_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restri
                   TilePartial *__restrict__ partials, TilePartial *__restrict__ gparts,
                   unsigned *__restrict__ gcount, BcTable *__restrict__ bct,
                   const CUtensorMap *__restrict__ maps) {
-  constexpr bool kAllValid = PATH == 1;
-  constexpr bool ALLV = kAllValid;
   using S = PairSmem<TY>;
-  constexpr int R = S::R;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   S &s = *reinterpret_cast<S *>(smem_raw);
-  const PairView<TY> V{s};
-  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  if (threadIdx.x == 0) {
+    mbar_init(&s.bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  unsigned phase = 0;
+  const int n_list = counts[PATH];
+  const int32_t *list = order + (PATH == 1 ? counts[0] : 0);
+  for (int k = blockIdx.x; k < n_list; k += gridDim.x)
+    if (!pair_tile<TY, SOURCES, PATH>(s, phase, list[k], insts, tile_inst, partials, gparts,
+                                      gcount, bct, maps))
+      return;
+}
+
+// ===========================================================================
+// The persistent step: every instance of a batch advanced by nsteps steps in
+// ONE cooperative launch of resident CTAs.  Per step, CTAs take tiles from a
+// global counter in the prepared order (general tiles first), each tile runs
+// exactly as in the per-step kernel (its instance's last tile finalizes the
+// clock), and a grid barrier ends the step.  The barrier wait is bounded by
+// `budget` clock cycles: a CTA that gives up sets the give-up flag and bit 8
+// of every instance's status and leaves, and every other CTA leaves at its
+// next wait when it sees the flag; nothing waits without bound.
+// sync[0] counts tile fetches (every CTA makes exactly one failed fetch per
+// step, so step k's fetches start at k * (n_tiles + gridDim.x)), sync[1] the
+// barrier arrivals, sync[2] is the give-up flag; the host zeroes them before
+// every launch.
+// ===========================================================================
+constexpr int kPersistMinBlocks = 4;
+
+// A general tile of the persistent step, kept out of line so that the
+// all-valid path inlined in the kernel gets the register allocation it gets in
+// its own build (the general path's ghost faces would otherwise cost it spills).
+template <int TY, bool SOURCES>
+__device__ __noinline__ bool pair_tile_general(PairSmem<TY> &s, unsigned &phase, const int tile,
+                                               const hb_instance *__restrict__ insts,
+                                               const int32_t *__restrict__ tile_inst,
+                                               TilePartial *__restrict__ partials,
+                                               TilePartial *__restrict__ gparts,
+                                               unsigned *__restrict__ gcount,
+                                               BcTable *__restrict__ bct,
+                                               const CUtensorMap *__restrict__ maps) {
+  return pair_tile<TY, SOURCES, 0>(s, phase, tile, insts, tile_inst, partials, gparts, gcount, bct,
+                                   maps);
+}
+
+template <int TY, bool SOURCES>
+__global__ void __launch_bounds__(kRowsNT, kPersistMinBlocks)
+pairs_persistent_kernel(const hb_instance *__restrict__ insts,
+                        const int32_t *__restrict__ tile_inst, const int32_t *__restrict__ order,
+                        const int32_t *__restrict__ counts, const uint8_t *__restrict__ allvalid,
+                        TilePartial *__restrict__ partials, TilePartial *__restrict__ gparts,
+                        unsigned *__restrict__ gcount, BcTable *__restrict__ bct,
+                        const CUtensorMap *__restrict__ maps, int n_instances, int nsteps,
+                        unsigned long long *__restrict__ sync, long long budget) {
+  using S = PairSmem<TY>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  S &s = *reinterpret_cast<S *>(smem_raw);
+  __shared__ unsigned long long s_tile;
+  __shared__ int s_stop;
+  const int tid = threadIdx.x;
   if (tid == 0) {
     mbar_init(&s.bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
   unsigned phase = 0;
-
-  const int n_list = counts[PATH];
-  const int32_t *list = order + (kAllValid ? counts[0] : 0);
-  for (int k = blockIdx.x; k < n_list; k += gridDim.x) {
-    const int tile = list[k];
-    const int ii = tile_inst[tile];
-    const hb_instance &in = insts[ii];
-    hb_ctrl *ctrl = in.ctrl;
-    if (ctrl->halted) continue;
-    const int lt = tile - in.tile_begin;
-    const int tyi = lt / in.tiles_x, txi = lt - tyi * in.tiles_x;
-    const int y0 = tyi * TY, x0 = txi * kPW;
-    const int cur = ctrl->cur;
-    const double t = ctrl->t;
-    const float dt = (float)ctrl->dt;
-    const float dx = (float)in.dx;
-    const float rain = (float)ctrl->rain_rate;
-    const bool first = (t == 0.0);
-    const int P = in.pitch;
-    const CUtensorMap *m = maps + (size_t)ii * kMapsPerInstance;
-
+  const unsigned long long n = (unsigned long long)(counts[0] + counts[1]);
+  const unsigned long long G = gridDim.x;
+  cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> fetches(sync[0]);
+  cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> arrivals(sync[1]);
+  cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> gave_up(sync[2]);
+  for (int step = 0; step < nsteps; ++step) {
+    const unsigned long long base = (unsigned long long)step * (n + G);
+    for (;;) {
+      if (tid == 0) s_tile = fetches.fetch_add(1ull, cuda::memory_order_relaxed) - base;
+      __syncthreads();
+      const unsigned long long k = s_tile;
+      __syncthreads();
+      if (k >= n) break;
+      const int tile = order[k];
+      const bool ok = allvalid[tile]
+                          ? pair_tile<TY, SOURCES, 1>(s, phase, tile, insts, tile_inst, partials,
+                                                      gparts, gcount, bct, maps)
+                          : pair_tile_general<TY, SOURCES>(s, phase, tile, insts, tile_inst,
+                                                           partials, gparts, gcount, bct, maps);
+      if (!ok) {
+        if (tid == 0) gave_up.fetch_or(1ull, cuda::memory_order_relaxed);
+        return;
+      }
+    }
+    // --- grid barrier: this step's state stores (generic proxy) before the
+    // next step's tile loads (TMA, async proxy) on any SM
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    __syncthreads();
     if (tid == 0) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_expect_tx(&s.bar, S::kTxBytes);
-      tma_load_2d(s.f[0], m + 0 + cur, x0, y0, &s.bar);
-      tma_load_2d(s.f[1], m + 2 + cur, x0, y0, &s.bar);
-      tma_load_2d(s.f[2], m + 4 + cur, x0, y0, &s.bar);
-      tma_load_2d(s.f[3], m + 6, x0, y0, &s.bar);
-      tma_load_2d(s.hmax, m + 7, x0 + HB_PAD_X, y0 + HB_PAD_Y, &s.bar);
-      tma_load_2d(s.code, m + 8, x0, y0, &s.bar);
-    }
-    if (tid < HB_MAX_CLASSES) {
-      if constexpr (!kAllValid) {
-        s.bctype[tid] = in.bc_type[tid];
-        for (int q = 0; q < 4; q++) s.bc[tid][q] = bct[ii].v[tid][q];
+      __threadfence();
+      arrivals.fetch_add(1ull, cuda::memory_order_release);
+      const unsigned long long target = (unsigned long long)(step + 1) * G;
+      const long long t0 = clock64();
+      int stop = 0;
+      while (arrivals.load(cuda::memory_order_acquire) < target) {
+        if (gave_up.load(cuda::memory_order_relaxed)) {
+          stop = 1;
+          break;
+        }
+        if (clock64() - t0 > budget) {
+          stop = 2;
+          break;
+        }
+        __nanosleep(64);
       }
-    } else if (tid >= 64 && tid < 64 + HB_MAX_ZONES) {
-      s.manning[tid - 64] = (float)in.manning[tid - 64];
-    }
-    const int bug_y = in.bug_y, bug_x = in.bug_x;
-    float datum_tile = 0.f;
-    if (in.datum) {
-      const int by = y0 / HB_DATUM_BLOCK, bx = x0 / HB_DATUM_BLOCK;
-      datum_tile = in.datum[by * in.datum_nx + bx];
-      if (tid >= 32 && tid < 41) {
-        const int q = tid - 32, dyb = q / 3 - 1, dxb = q % 3 - 1;
-        const int yy = min(max(by + dyb, 0), in.datum_ny - 1);
-        const int xx = min(max(bx + dxb, 0), in.datum_nx - 1);
-        s.ddatum[q] = in.datum[yy * in.datum_nx + xx] - datum_tile;
+      // the last block to arrive skips the wait: it stops too if any block
+      // gave up, so that no block carries on alone
+      if (!stop && gave_up.load(cuda::memory_order_relaxed)) stop = 1;
+      if (stop == 2) {
+        gave_up.fetch_or(1ull, cuda::memory_order_relaxed);
+        for (int i = 0; i < n_instances; i++) atomicOr(&insts[i].ctrl->status, 8);
       }
-    }
-    const bool arrived = mbar_wait(&s.bar, phase, 4000000000LL);
-    if (__syncthreads_or(!arrived)) {
-      if (tid == 0) atomicOr(&ctrl->status, 2);
-      mbar_wait(&s.bar, phase, 4000000000LL);
-      return;
-    }
-    phase ^= 1u;
-    if (in.datum) {
-      __syncthreads();  // ddatum visible
-      const int by0 = (y0 / HB_DATUM_BLOCK) * HB_DATUM_BLOCK;
-      const int bx0 = (x0 / HB_DATUM_BLOCK) * HB_DATUM_BLOCK;
-      const DatumHalo dh = datum_halo(y0, x0, by0, bx0, TY, kPW, kPSWF, HB_DATUM_BLOCK);
-      const int NH = dh.count();
-      for (int q = tid; q < NH; q += kRowsNT) {
-        int i, j;
-        datum_halo_cell(dh, q, TY, kPW, kPSWF, i, j);
-        const int ry = y0 + i, rx = x0 + j;
-        const int dyb = ry < by0 ? 0 : (ry >= by0 + HB_DATUM_BLOCK ? 2 : 1);
-        const int dxb = rx < bx0 ? 0 : (rx >= bx0 + HB_DATUM_BLOCK ? 2 : 1);
-        if (dyb != 1 || dxb != 1) s.f[3][V.fi(i, j)] += s.ddatum[dyb * 3 + dxb];
-      }
+      asm volatile("fence.proxy.async.global;" ::: "memory");
+      s_stop = stop;
     }
     __syncthreads();
-
-    // --- tile edges: warp 0 the faces between columns 63 | 64 (east faces of
-    // lane 31's second cell), two rows per lane; warp 1 the x-slopes of
-    // column -1 (west neighbour of lane 0's first cell)
-    if (w == 0) {
-      for (int i = 2 * lane; i < TY; i += 64) {
-        float a[4], b[4];  // slopes of col 63 / col 64 for rows i, i + 1 (h, z, qx, qy)
-        float a1[4], b1[4];
-        xslope1<TY, ALLV>(V, i, 63, a[0], a[1], a[2], a[3]);
-        xslope1<TY, ALLV>(V, i + 1, 63, a1[0], a1[1], a1[2], a1[3]);
-        xslope1<TY, ALLV>(V, i, 64, b[0], b[1], b[2], b[3]);
-        xslope1<TY, ALLV>(V, i + 1, 64, b1[0], b1[1], b1[2], b1[3]);
-        const Slp2 sA{pk(a[0], a1[0]), pk(a[1], a1[1]), pk(a[2], a1[2]), pk(a[3], a1[3])};
-        const Slp2 sB{pk(b[0], b1[0]), pk(b[1], b1[1]), pk(b[2], b1[2]), pk(b[3], b1[3])};
-        const Fc2 f = face_pair<0, ALLV>(s, V.vpair(i, 63), V.vpair(i, 64), sA, sB,
-                                         V.code(i, 63), V.code(i + 1, 63), V.code(i, 64),
-                                         V.code(i + 1, 64), datum_tile);
-        s.xe[i][0] = f.fh.x; s.xe[i][1] = f.fx.x; s.xe[i][2] = f.fy.x; s.xe[i][3] = f.sa.x;
-        s.xe[i + 1][0] = f.fh.y; s.xe[i + 1][1] = f.fx.y; s.xe[i + 1][2] = f.fy.y;
-        s.xe[i + 1][3] = f.sa.y;
-      }
-    } else if (w == 1) {
-      for (int i = lane; i < TY; i += 32) {
-        float sh, sz, sqx, sqy;
-        xslope1<TY, ALLV>(V, i, -1, sh, sz, sqx, sqy);
-        s.sxw[i][0] = sh;
-        s.sxw[i][1] = sz;
-        s.sxw[i][2] = sqx;
-        s.sxw[i][3] = sqy;
-      }
-    }
-
-    const int r0 = w * R;
-    const int j0 = 2 * lane;  // this lane's first column
-    const int rx0 = x0 + j0;
-    f2 vol2 = dup(0.f);
-    float smax_t = 0.f;
-    double outf = 0.0;
-    int any_dry = 0;
-    {
-      // validity of a pair as two floats (1 valid, 0 not); all-valid: 1
-      auto vpair = [&](int i) -> f2 {
-        if constexpr (ALLV) {
-          (void)i;
-          return dup(1.f);
-        } else {
-          return pk(is_valid(V.code(i, j0)) ? 1.f : 0.f, is_valid(V.code(i, j0 + 1)) ? 1.f : 0.f);
-        }
-      };
-      // --- column window of the pair: row r0 and its y-slopes, the face
-      // between rows r0-1 and r0, the depths of row r0-1
-      Cel2 C = V.pair(r0, j0);
-      f2 vC = vpair(r0), vN = vpair(r0 - 1);
-      f2 Nh;
-      Slp2 syC;
-      Fc2 nf;
-      {
-        const Cel2 N = V.pair(r0 - 1, j0), NN = V.pair(r0 - 2, j0), S1 = V.pair(r0 + 1, j0);
-        const Slp2 syN = yslope2<ALLV>(N, C, vC, NN, vpair(r0 - 2));
-        syC = yslope2<ALLV>(C, S1, vpair(r0 + 1), N, vN);
-        // face between rows r0-1 (north, B) and r0 (south, A)
-        nf = face_pair<1, ALLV>(s, C, N, syC, syN, V.code(r0, j0), V.code(r0, j0 + 1),
-                                V.code(r0 - 1, j0), V.code(r0 - 1, j0 + 1), datum_tile);
-        Nh = N.h;
-      }
-      __syncthreads();  // tile-edge faces and slopes ready
-      float *hout = (float *)in.h[1 - cur];
-      float *qxout = (float *)in.qx[1 - cur];
-      float *qyout = (float *)in.qy[1 - cur];
-      float *hmaxg = (float *)in.h_max;
-      const bool infil = SOURCES && in.cum != nullptr;
-      const bool stations = SOURCES && in.rain_station != nullptr;
-      const bool fwd_tile = (y0 < HB_PAD_Y && in.halo_up[0] != nullptr) ||
-                            (y0 + TY > in.rows - HB_PAD_Y && in.halo_down[0] != nullptr);
-      const f2 r2 = dup(dt / dx);
-      const float rdt = rain * dt;
-      const float dtg = dt * kGF;
-
-#pragma unroll 1
-      for (int i = r0; i < r0 + R; ++i) {
-        // --- x-direction: neighbours W (col 2j-1) and E (col 2j+2)
-        const int kc = V.fi(i, j0);
-        float Wv[4], Ev[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          Wv[q] = s.f[q][kc - 1];
-          Ev[q] = s.f[q][kc + 2];
-        }
-        uint8_t kW = 0, kE = 0;
-        const uint8_t kA = V.code(i, j0), kB = V.code(i, j0 + 1);
-        bool vWb = true, vAb = true, vBb = true, vEb = true;
-        if constexpr (!ALLV) {
-          kW = V.code(i, j0 - 1);
-          kE = V.code(i, j0 + 2);
-          vWb = is_valid(kW);
-          vAb = is_valid(kA);
-          vBb = is_valid(kB);
-          vEb = is_valid(kE);
-        }
-        // x-slopes of cells a = 2j and b = 2j+1 (fields h, qx, qy, z)
-        const float cA[4] = {C.h.x, C.qx.x, C.qy.x, C.z.x};
-        const float cB[4] = {C.h.y, C.qx.y, C.qy.y, C.z.y};
-        float sxa[4], sxb[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          sxa[q] = slope1(cA[q], vWb ? Wv[q] : cA[q], vBb ? cB[q] : cA[q]);
-          sxb[q] = slope1(cB[q], vAb ? cA[q] : cB[q], vEb ? Ev[q] : cB[q]);
-        }
-        // slope of col 2j-1 from the west lane (lane 0: the pre-pass)
-        float sw[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) sw[q] = __shfl_up_sync(0xffffffffu, sxb[q], 1);
-        if (lane == 0) {
-          sw[0] = s.sxw[i][0];
-          sw[3] = s.sxw[i][1];
-          sw[1] = s.sxw[i][2];
-          sw[2] = s.sxw[i][3];
-        }
-        // --- west faces of a and b: (2j-1 | 2j) and (2j | 2j+1)
-        f2 Px_h, Px_x, Px_y;  // x-direction flux differences (west - east) of the pair
-        f2 wfh;               // west-face mass flux (outflow of boundary faces)
-        f2 efh;               // east-face mass flux
-        {
-          const Cel2 Aw{pk(Wv[0], C.h.x), pk(Wv[1], C.qx.x), pk(Wv[2], C.qy.x), pk(Wv[3], C.z.x)};
-          const Slp2 sAw{pk(sw[0], sxa[0]), pk(sw[3], sxa[3]), pk(sw[1], sxa[1]), pk(sw[2], sxa[2])};
-          const Slp2 sBw{pk(sxa[0], sxb[0]), pk(sxa[3], sxb[3]), pk(sxa[1], sxb[1]), pk(sxa[2], sxb[2])};
-          const Fc2 wf = face_pair<0, ALLV>(s, Aw, C, sAw, sBw, kW, kA, kA, kB, datum_tile);
-          // east faces: a's is the lane's second west face; b's comes from lane j+1
-          float e_h = __shfl_down_sync(0xffffffffu, wf.fh.x, 1);
-          float e_x = __shfl_down_sync(0xffffffffu, wf.fx.x, 1);
-          float e_y = __shfl_down_sync(0xffffffffu, wf.fy.x, 1);
-          float e_a = __shfl_down_sync(0xffffffffu, wf.sa.x, 1);
-          if (lane == 31) {
-            e_h = s.xe[i][0];
-            e_x = s.xe[i][1];
-            e_y = s.xe[i][2];
-            e_a = s.xe[i][3];
-          }
-          const f2 ef_h = pk(wf.fh.y, e_h), ef_x = pk(wf.fx.y, e_x), ef_y = pk(wf.fy.y, e_y),
-                   ef_a = pk(wf.sa.y, e_a);
-          Px_h = sub2(wf.fh, ef_h);
-          Px_x = add2(sub2(sub2(wf.fx, ef_x), ef_a), wf.sb);
-          Px_y = sub2(wf.fy, ef_y);
-          wfh = wf.fh;
-          efh = ef_h;
-        }
-        // --- the row below, its y-slopes, and the south faces: rows i+1 (A) | i (B)
-        const Cel2 Sx = V.pair(i + 1, j0);
-        const f2 vS = vpair(i + 1);
-        Fc2 sf;
-        Slp2 syS;
-        {
-          const Cel2 SS = V.pair(i + 2, j0);
-          syS = yslope2<ALLV>(Sx, SS, vpair(i + 2), C, vC);
-          uint8_t kSa = 0, kSb = 0;
-          if constexpr (!ALLV) {
-            kSa = V.code(i + 1, j0);
-            kSb = V.code(i + 1, j0 + 1);
-          }
-          sf = face_pair<1, ALLV>(s, Sx, C, syS, syC, kSa, kSb, kA, kB, datum_tile);
-        }
-
-        // --- cell updates
-        const int ry = y0 + i;
-        // fluxMask activity (HC/fluxMaskGenerator_Kernel.cu:19-42)
-        bool act0 = first || C.h.x > kHsF, act1 = first || C.h.y > kHsF;
-        if (!(act0 && act1)) {
-          if constexpr (ALLV) {
-            act0 = act0 || C.h.y > kHsF || Nh.x > kHsF || Wv[0] > kHsF || Sx.h.x > kHsF;
-            act1 = act1 || Ev[0] > kHsF || Nh.y > kHsF || C.h.x > kHsF || Sx.h.y > kHsF;
-          } else {
-            const int ra = rx0, rb = rx0 + 1;
-            auto nb = [&](bool v, int yy, int xx, float hh) {
-              return v && !(yy == bug_y && xx == bug_x) && hh > kHsF;
-            };
-            act0 = act0 || nb(vBb, ry, ra + 1, C.h.y) || nb(vN.x != 0.f, ry - 1, ra, Nh.x) ||
-                   nb(vWb, ry, ra - 1, Wv[0]) || nb(vS.x != 0.f, ry + 1, ra, Sx.h.x);
-            act1 = act1 || nb(vEb, ry, rb + 1, Ev[0]) || nb(vN.y != 0.f, ry - 1, rb, Nh.y) ||
-                   nb(vAb, ry, rb - 1, C.h.x) || nb(vS.y != 0.f, ry + 1, rb, Sx.h.y);
-          }
-        }
-        f2 hu = mul2(add2(Px_h, sub2(sf.fh, nf.fh)), r2);
-        f2 qxu = mul2(add2(Px_x, sub2(sf.fx, nf.fx)), r2);
-        f2 qyu = mul2(add2(Px_y, add2(sub2(sub2(sf.fy, nf.fy), nf.sa), sf.sb)), r2);
-        if (!act0) hu.x = qxu.x = qyu.x = 0.f;
-        if (!act1) hu.y = qxu.y = qyu.y = 0.f;
-        if constexpr (!ALLV) {
-          // outflow through boundary faces of active valid cells
-          const bool bE0 = !vBb, bW0 = !vWb, bN0 = vN.x == 0.f, bS0 = vS.x == 0.f;
-          const bool bE1 = !vEb, bW1 = !vAb, bN1 = vN.y == 0.f, bS1 = vS.y == 0.f;
-          if (vAb && act0 && (bE0 | bW0 | bN0 | bS0)) {
-            double o = 0.0;
-            if (bE0) o += (double)efh.x;
-            if (bN0) o += (double)nf.fh.x;
-            if (bW0) o -= (double)wfh.x;
-            if (bS0) o -= (double)sf.fh.x;
-            outf += o;
-          }
-          if (vBb && act1 && (bE1 | bW1 | bN1 | bS1)) {
-            double o = 0.0;
-            if (bE1) o += (double)efh.y;
-            if (bN1) o += (double)nf.fh.y;
-            if (bW1) o -= (double)wfh.y;
-            if (bS1) o -= (double)sf.fh.y;
-            outf += o;
-          }
-        }
-        // rain (HP/SWE_CUDA.py:549 / HC/stationPrecipitation_Kernel.cu:27)
-        const size_t go = (size_t)(ry + HB_PAD_Y) * P + (rx0 + HB_PAD_X);
-        if (stations) {
-          hu.x += (float)in.station_rate[in.rain_station[go]] * dt;
-          hu.y += (float)in.station_rate[in.rain_station[go + 1]] * dt;
-        } else {
-          hu = add2(hu, dup(rdt));
-        }
-        if (infil) {
-          // Green-Ampt infiltration on the active cells, after rain
-          // (HC/infiltrationCUDA_Kernel.cu:20-46; order HP/CatchFlood_main.py:164-170)
-#pragma unroll
-          for (int c = 0; c < 2; c++) {
-            const bool act = c ? act1 : act0;
-            const bool vc = c ? vBb : vAb;
-            if (!(act && vc)) continue;
-            const uint8_t kc_ = c ? kB : kA;
-            const float hc = c ? C.h.y : C.h.x;
-            float *cum = (float *)in.cum + go + c;
-            const int zc = kc_ & 15;
-            const float K = (float)in.ks[zc], psi = (float)in.psi[zc], dth = (float)in.dtheta[zc];
-            const float F0 = *cum;
-            const float a = F0 + dt * K;
-            const float F1 = 0.5f * (a + sqrtf(a * a + 4.f * dt * K * (psi + hc) * dth));
-            const float dF = fminf(hc, F1 - F0);
-            *cum = F0 + dF;
-            if (c) hu.y -= dF; else hu.x -= dF;
-          }
-        }
-        // implicit friction + update (HC/friction_implicit_andUpdate_jh_Kernel.cu:22-146)
-        const f2 h2 = add2(C.h, hu);
-        f2 qx2 = add2(C.qx, qxu), qy2 = add2(C.qy, qyu);
-        f2 sgh = dup(0.f), ih = dup(0.f);
-        const f2 nman = pk(s.manning[kA & 15], s.manning[kB & 15]);
-        {
-          const f2 gh = mul2(dup(kGF), h2);
-          sgh = pk(sqrta(gh.x), sqrta(gh.y));
-          ih = pk(rcpa(h2.x), rcpa(h2.y));
-          const f2 qq = fma2(qx2, qx2, mul2(qy2, qy2));
-          const f2 qn = pk(sqrta(qq.x), sqrta(qq.y));
-          const f2 cb = pk(ex2a(lg2a(h2.x) * (-1.f / 3.f)), ex2a(lg2a(h2.y) * (-1.f / 3.f)));
-          const f2 a = mul2(mul2(mul2(mul2(mul2(dup(dtg), nman), nman), cb), ih), ih);
-          const f2 sq = fma2(mul2(dup(4.f), a), qn, dup(1.f));
-          const f2 den = add2(dup(1.f), pk(sqrta(sq.x), sqrta(sq.y)));
-          const f2 fct = pk(2.f * rcpa(den.x), 2.f * rcpa(den.y));
-          const f2 lim = mul2(mul2(dup(5.f), h2), sgh);
-          const f2 tx = mul2(qx2, fct), ty = mul2(qy2, fct);
-#pragma unroll
-          for (int c = 0; c < 2; c++) {
-            const float hh = c ? h2.y : h2.x;
-            float &qx = c ? qx2.y : qx2.x;
-            float &qy = c ? qy2.y : qy2.x;
-            if (hh < kHsF) {
-              qx = 0.f;
-              qy = 0.f;
-              if (c) { sgh.y = 0.f; ih.y = 0.f; } else { sgh.x = 0.f; ih.x = 0.f; }
-              continue;
-            }
-            if (!((c ? nman.y : nman.x) > 0.f)) continue;
-            const float l = c ? lim.y : lim.x;
-            if (fabsf(qx) > 1.0e-10f) {
-              const float temp = c ? tx.y : tx.x;
-              if (fabsf(temp) > l) {
-                const float q2 = 2.f * temp - qx;
-                qx = (q2 * temp <= 0.f) ? 0.f : q2;
-              } else {
-                qx = temp;
-              }
-            }
-            if (fabsf(qy) > 1.0e-10f) {
-              const float temp = c ? ty.y : ty.x;
-              if (fabsf(temp) > l) {
-                const float q2 = 2.f * temp - qy;
-                qy = (q2 * temp <= 0.f) ? 0.f : q2;
-              } else {
-                qy = temp;
-              }
-            }
-          }
-        }
-        // stores: both cells valid (every all-valid tile), else per cell
-        const f2 hm_old = *reinterpret_cast<const f2 *>(&s.hmax[i * kPW + j0]);
-        const f2 hm = pk(fmaxf(h2.x, hm_old.x), fmaxf(h2.y, hm_old.y));
-        if (vAb && vBb) {
-          *reinterpret_cast<f2 *>(hout + go) = h2;
-          *reinterpret_cast<f2 *>(qxout + go) = qx2;
-          *reinterpret_cast<f2 *>(qyout + go) = qy2;
-          *reinterpret_cast<f2 *>(hmaxg + go) = hm;
-        } else {
-          if (vAb) {
-            hout[go] = h2.x; qxout[go] = qx2.x; qyout[go] = qy2.x; hmaxg[go] = hm.x;
-          }
-          if (vBb) {
-            hout[go + 1] = h2.y; qxout[go + 1] = qx2.y; qyout[go + 1] = qy2.y; hmaxg[go + 1] = hm.y;
-          }
-        }
-        if (fwd_tile) {
-          const int ob = 1 - cur;
-          auto fwd = [&](void *const *dst, int row) {
-            const size_t gh = (size_t)row * P + (rx0 + HB_PAD_X);
-            if (vAb) {
-              ((float *)dst[ob])[gh] = h2.x;
-              ((float *)dst[2 + ob])[gh] = qx2.x;
-              ((float *)dst[4 + ob])[gh] = qy2.x;
-            }
-            if (vBb) {
-              ((float *)dst[ob])[gh + 1] = h2.y;
-              ((float *)dst[2 + ob])[gh + 1] = qx2.y;
-              ((float *)dst[4 + ob])[gh + 1] = qy2.y;
-            }
-          };
-          if (ry < HB_PAD_Y && in.halo_up[0] != nullptr)
-            fwd(in.halo_up, in.halo_up_rows + HB_PAD_Y + ry);
-          if (ry >= in.rows - HB_PAD_Y && in.halo_down[0] != nullptr)
-            fwd(in.halo_down, ry - in.rows + HB_PAD_Y);
-          // the neighbour may be a peer GPU: order these stores system-wide
-          // before this tile's partial, its group count and the host's next
-          // collective
-          __threadfence_system();
-        }
-        // CFL speed (HC/timeControl_Kernel.cu:186-189), volume
-        const f2 sp = fma2(pk(fmaxf(fabsf(qx2.x), fabsf(qy2.x)), fmaxf(fabsf(qx2.y), fabsf(qy2.y))),
-                           ih, sgh);
-        if (vAb) {
-          if (h2.x > kHsF) smax_t = fmaxf(smax_t, sp.x); else any_dry = 1;
-        }
-        if (vBb) {
-          if (h2.y > kHsF) smax_t = fmaxf(smax_t, sp.y); else any_dry = 1;
-        }
-        vol2 = add2(vol2, pk(vAb ? h2.x : 0.f, vBb ? h2.y : 0.f));
-
-        // slide the column window down one row
-        nf = sf;
-        Nh = C.h;
-        vN = vC;
-        C = Sx;
-        vC = vS;
-        syC = syS;
-      }
-    }
-
-    // --- tile partials and the instance's last-tile finalize
-    double vol = warp_sum((double)vol2.x + (double)vol2.y);
-    if constexpr (!kAllValid) outf = warp_sum(outf);
-    const double smax = (double)warp_max(smax_t);
-    any_dry = __any_sync(0xffffffffu, any_dry);
-    if (lane == 0) {
-      s.red_d[0][w] = vol;
-      s.red_d[1][w] = outf;
-      s.red_s[w] = smax;
-      s.red_i[w] = any_dry;
-    }
-    __syncthreads();
-    const int n_inst_tiles = in.tiles_x * in.tiles_y;
-    const int grp = lt / kGroupTiles;
-    const int gsize = min(kGroupTiles, n_inst_tiles - grp * kGroupTiles);
-    const int gbase = in.tile_begin / kGroupTiles + ii;
-    if (tid == 0) {
-      TilePartial p;
-      p.volume = p.outflow = p.smax = 0.0;
-      p.any_dry = 0;
-      p.pad = 0;
-      for (int q = 0; q < kRowsNW; q++) {
-        p.volume += s.red_d[0][q];
-        p.outflow += s.red_d[1][q];
-        p.smax = fmax(p.smax, s.red_s[q]);
-        p.any_dry |= s.red_i[q];
-      }
-      partials[tile] = p;
-      cuda::atomic_ref<unsigned, cuda::thread_scope_device> done(gcount[gbase + grp]);
-      s.last = (done.fetch_add(1u, cuda::memory_order_acq_rel) == (unsigned)(gsize - 1));
-    }
-    __syncthreads();
-    if (s.last)
-      close_group<float, kRowsNT>(in, ii, partials + in.tile_begin + grp * kGroupTiles, gsize,
-                                  gparts, gcount, gbase + grp, gbase,
-                                  (n_inst_tiles + kGroupTiles - 1) / kGroupTiles, bct, s.red_d,
-                                  s.red_s, s.red_i, &s.last2);
-    __syncthreads();
+    if (s_stop) return;
   }
 }

@@ -115,6 +115,7 @@ SIGNATURES = {
     "hb_fused_workspace_size": (ctypes.c_size_t, [_P]),
     "hb_fused_prepare": (_I, [_P, _P]),
     "hb_fused_step": (_I, [_P, _I, _P]),
+    "hb_fused_run": (_I, [_P, _I, ctypes.c_longlong, _P]),
     "hb_fused_step_noalloc": (_I, [_P, _I, _I, _P]),
     "hb_fused_finish": (_I, [_P, _P, _P]),
     "hb_adjoint_step": (_I, [_P, _P]),

@@ -1,7 +1,8 @@
 """Autotuner for the fused step's launch shape.
 
-For a batch of catchments it times a few steps of each candidate (tile height
-and resident-CTA count) on scratch copies of the catchments, keeps the fastest,
+For a batch of catchments it times a few steps of each candidate (cells per
+lane -- 2 with 32 x 64 tiles, 1 with 32 x 32 or 64 x 32 tiles -- tile height and
+resident-CTA count) on scratch copies of the catchments, keeps the fastest,
 and caches the choice in a JSON file keyed by the GPU name, the dtype and the
 batch's shape (number of instances, total cells, largest side).  The cache
 lives at $HIPIMS_B200_TUNE_CACHE, default ~/.cache/hipims_b200/autotune.json.
@@ -16,9 +17,14 @@ import torch
 
 from .fused import Catchment, FusedSolver
 
-DEFAULT_CANDIDATES = ({"tile": (64, 32)}, {"tile": (64, 32), "minb": 4},
-                      {"tile": (32, 32)}, {"tile": (32, 32), "minb": 5},
+# tile = (rows, cols); cols / 32 cells per lane
+DEFAULT_CANDIDATES = ({"tile": (32, 64), "minb": 4}, {"tile": (32, 64), "minb": 3},
+                      {"tile": (64, 32), "minb": 4}, {"tile": (32, 32), "minb": 5},
                       {"tile": (32, 32), "minb": 6})
+
+
+def cells_per_lane(cfg: dict) -> int:
+    return int(cfg["tile"][1]) // 32
 
 
 def cache_path() -> str:

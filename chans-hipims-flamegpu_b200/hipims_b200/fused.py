@@ -399,6 +399,33 @@ class FusedSolver:
                                                         1 if prepare else 0, self._stream()),
                        "hb_fused_step_noalloc")
 
+    def run_persistent(self, nsteps: int = 1, budget_cycles: int = 0) -> None:
+        """Enqueue nsteps steps of every instance as ONE persistent cooperative
+        launch (hb_fused_run; FP32 2nd order, 32 x 64 tiles): the same results
+        as step(nsteps).  budget_cycles bounds every grid-barrier wait (0: the
+        library's default, about a second); a wait that gives up sets status
+        bit 8, which check() reports."""
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.lib().hb_fused_run(ctypes.byref(self.batch), int(nsteps),
+                                               int(budget_cycles), self._stream()),
+                       "hb_fused_run")
+
+    def capture_persistent(self, nsteps: int) -> None:
+        """Capture one persistent launch of nsteps steps in a CUDA graph for
+        replay()."""
+        self._graph = None
+        torch.cuda.synchronize(self.device)
+        s = torch.cuda.Stream(self.device)
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                _lib.check(_lib.lib().hb_fused_run(ctypes.byref(self.batch), int(nsteps), 0,
+                                                   s.cuda_stream), "hb_fused_run")
+        torch.cuda.current_stream(self.device).wait_stream(s)
+        self._graph = g
+        self._graph_steps = nsteps
+
     def capture(self, nsteps: int) -> None:
         """Capture nsteps steps in a CUDA graph for replay()."""
         self._graph = None
@@ -432,7 +459,8 @@ class FusedSolver:
         self.ctrl.copy_(torch.frombuffer(bytearray(arr), dtype=torch.uint8))
 
     STATUS = {1: "non-finite time step", 2: "a tile's data did not arrive in time",
-              4: "non-finite depth"}
+              4: "non-finite depth",
+              8: "a grid barrier of the persistent step gave up (budget exhausted)"}
 
     def check(self) -> None:
         """Raise if a step flagged a failure in any control block (syncs)."""

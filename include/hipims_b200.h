@@ -133,6 +133,18 @@ size_t hb_fused_workspace_size(const struct hb_fused_batch *batch);
 int hb_fused_prepare(const struct hb_fused_batch *batch, void *stream);
 /* Enqueue `nsteps` fused steps (graph-capturable; no host sync). */
 int hb_fused_step(const struct hb_fused_batch *batch, int nsteps, void *stream);
+/* The same `nsteps` steps of every instance in ONE persistent cooperative
+ * launch (no reference counterpart; the ensemble form of the step): resident
+ * blocks take tiles from a counter, the instance's last tile advances its
+ * clock, and a grid barrier separates the steps.  Results equal nsteps calls
+ * of hb_fused_step bit for bit.  Built for FP32 2nd-order batches with
+ * 32 x 64 tiles (not for strips, whose clock needs hb_fused_finish between
+ * steps).  Every barrier wait gives up after budget_cycles SM clock cycles
+ * (<= 0: 2^31, about a second): the blocks then leave, bit 8 is set in every
+ * instance's status and the state is incomplete (re-prepare or restore before
+ * stepping on).  Needs hb_fused_prepare first; graph-capturable. */
+int hb_fused_run(const struct hb_fused_batch *batch, int nsteps, long long budget_cycles,
+                 void *stream);
 /* Clock advance of instances stepped with hb_ctrl.external_dt set (no
  * counterpart in the reference; one catchment split into row strips over
  * several instances or GPUs): ext = device [n_instances][2], the largest wave

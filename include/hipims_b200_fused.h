@@ -70,7 +70,8 @@ typedef struct hb_ctrl {
   int32_t rain_index;    /* monotone cursor into the rain table */
   uint32_t tiles_done;   /* internal last-tile-done counter */
   int32_t status;        /* bits: 1 non-finite dt, 2 a tile's data did not arrive
-                            (TMA wait timed out), 4 non-finite depth (FP64 volume) */
+                            (TMA wait timed out), 4 non-finite depth (FP64 volume),
+                            8 a grid barrier of hb_fused_run gave up (budget) */
   float bc_vals[HB_MAX_CLASSES][4]; /* given h, wl, qx, qy per class at t */
   /* Deferred time step (strips of one catchment on several instances or
    * GPUs): with external_dt set, a step leaves dt, t, the step counter and
