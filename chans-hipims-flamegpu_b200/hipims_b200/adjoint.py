@@ -22,6 +22,13 @@ that the nonlinear step saturates, so the exact adjoint through such cells
 grows without bound while the loss stays smooth.  Masking them drops only the
 sensitivity carried by sub-0.01 mm films; h_reg = 0 masks negative depths
 only.
+With ``forward_dtype=torch.float32`` the forward, its checkpoints and the
+recomputed segments run in the FP32 product (the two-cells-per-lane step), and
+the reverse sweep linearises the FP64 step at those FP32 states: the
+gradient of the loss the FP32 run computes, to within the FP32 trajectory's
+distance from FP64.  Its FP64 reference gradient is the same problem with
+``forward_dtype=torch.float64``.
+
 The reference has no adjoint; the forward it differentiates is the reference
 step (HP/SWE_CUDA.py:339-424 with HC/fluxCal_2ndOrder_jh_improved_Kernel.cu,
 HC/friction_implicit_andUpdate_jh_Kernel.cu and HP/SWE_CUDA.py:472-495 for rain).
@@ -77,7 +84,8 @@ class GaugeMisfit:
     def __init__(self, catchment: Catchment, gauge_rows, gauge_cols, nsteps: int,
                  dt_schedule: np.ndarray, every: int = 10, checkpoint: int = 100,
                  obs=None, weight: float = 1.0, h_reg: float = 1.0e-5,
-                 store_faces: bool = True, device="cuda"):
+                 store_faces: bool = True, device="cuda",
+                 forward_dtype: torch.dtype = torch.float64):
         dts = np.asarray(dt_schedule, dtype=np.float64)
         if dts.shape[0] < nsteps:
             raise ValueError(f"dt schedule has {dts.shape[0]} steps, {nsteps} needed")
@@ -92,7 +100,14 @@ class GaugeMisfit:
         self.weight = float(weight)
         self.h_reg = float(h_reg)
         self.store_faces = bool(store_faces)
-        self.fs = FusedSolver(self.catchment, dtype=torch.float64, device=device)
+        if forward_dtype not in (torch.float32, torch.float64):
+            raise ValueError("forward_dtype must be float32 or float64")
+        self.forward_dtype = forward_dtype
+        self.fs = FusedSolver(self.catchment, dtype=forward_dtype, device=device)
+        # the reverse sweep reads the FP64 instance record (bed, codes, tables)
+        # and FP64 states on the same dense layout
+        self.fs64 = self.fs if forward_dtype == torch.float64 else FusedSolver(
+            self.catchment, dtype=torch.float64, device=device)
         self.device = self.fs.device
         self.n_zones = len(catchment.manning)
         self.offsets = self.fs.cell_offsets(0, np.asarray(gauge_rows), np.asarray(gauge_cols))
@@ -124,6 +139,8 @@ class GaugeMisfit:
         the checkpoints for gradient()."""
         self._params = ([float(v) for v in manning], float(rain_mult))
         self.fs.set_manning(0, self._params[0])
+        if self.fs64 is not self.fs:
+            self.fs64.set_manning(0, self._params[0])
         self.fs.reset(rain_mult=self._params[1])
         samples = torch.empty(self.n_samples, self.n_gauges, dtype=torch.float64,
                               device=self.device)
@@ -140,7 +157,7 @@ class GaugeMisfit:
             if k % self.K == 0 and k < self.nsteps:
                 h, qx, qy = self._state(k)
                 self._ckpt[k] = (torch.stack([h, qx, qy]), self.fs.ctrl.clone())
-        self._h_last = self._state(self.nsteps)[0].clone()
+        self._h_last = self._state(self.nsteps)[0].double().clone()
         self.samples = samples
         return samples
 
@@ -165,7 +182,7 @@ class GaugeMisfit:
                              device=dev)
         ctrl_log = torch.empty(min(self.K, self.nsteps), _CTRL_DOUBLES, dtype=torch.float64,
                                device=dev)
-        ins = self.fs.inst[0]
+        ins = self.fs64.inst[0]
         stream = torch.cuda.current_stream(dev).cuda_stream
         rain = self.catchment.rain
         w = self.weight
@@ -178,7 +195,7 @@ class GaugeMisfit:
         if self.nsteps % self.every == 0 and self.nsteps > 0:
             gauge(self._h_last, self.nsteps, lam[0])
         a = _lib.HbAdjointArgs()
-        a.instance = self.fs.record_ptr(0)
+        a.instance = self.fs64.record_ptr(0)
         a.rows, a.cols, a.pitch, a.code_pitch = ins.rows, ins.cols, ins.pitch, ins.code_pitch
         a.mu, a.mu_stride, a.grad = mu.data_ptr(), n, grad.data_ptr()
         a.h_reg = self.h_reg

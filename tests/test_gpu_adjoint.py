@@ -150,7 +150,7 @@ def test_dry_start_rain_case(cuda):
     128 x 128, 300 steps): the misfit is zero at the true parameters, the
     gradient is finite, and it matches central differences on every
     parameter whose difference quotient is resolvable (the same at relative
-    steps 1e-4 and 1e-5); most are."""
+    steps 1e-4, 1e-5 and 1e-6) to the north-star 1e-4; most are."""
     d = S.adjoint_case(128, seed=0, n_zones=8, n_gauges=16)
     c = S.catchment_from(d, t_end=math.inf)
     steps = 300
@@ -179,12 +179,17 @@ def test_dry_start_rain_case(cuda):
                 out.append((_J(q, start, 0.8 + e) - _J(q, start, 0.8 - e)) / (2 * e))
         return np.array(out)
 
-    f4, f5 = fd(1e-4), fd(1e-5)
+    # resolvable: the quotients agree across relative steps 1e-4, 1e-5 and
+    # 1e-6; where the loss jumps (a threshold crossed inside the step) they
+    # differ by factors and the branch derivative has nothing to match
+    f4, f5, f6 = fd(1e-4), fd(1e-5), fd(1e-6)
     scale = np.abs(f5).max()
-    stable = np.abs(f4 - f5) <= 1e-4 * scale
-    assert stable.sum() >= (len(g) + 1) // 2, (f4, f5)
+    stable = (np.abs(f4 - f5) <= 1e-4 * scale) & (np.abs(f6 - f5) <= 1e-4 * scale)
+    assert stable.sum() >= (len(g) + 1) // 2, (f4, f5, f6)
     err = np.abs(g - f5)[stable] / scale
-    assert err.max() <= 1e-3, (g, f5, stable)
+    print("dry-start adjoint vs central differences on", int(stable.sum()), "of", len(g),
+          "parameters: max err / max |fd| =", err.max())
+    assert err.max() <= GRAD_RTOL, (g, f5, stable)
 
 
 def test_face_scratch_gives_the_same_gradient(case, cuda):
@@ -202,3 +207,25 @@ def test_face_scratch_gives_the_same_gradient(case, cuda):
     for f in ("h", "qx", "qy"):
         a, b = lp[f].cpu().numpy(), lq[f].cpu().numpy()
         np.testing.assert_allclose(a, b, rtol=0, atol=1e-12 * np.abs(b).max())
+
+
+def test_fp32_forward_gradient_against_the_fp64_reference_gradient(case, cuda):
+    """The gradient along the FP32 product's trajectory (FP32 forward and
+    recompute, FP64 reverse sweep at those states) against the FP64 adjoint of
+    the same problem: the FP32 run's parameters carry the same sensitivity to
+    within its distance from the FP64 trajectory."""
+    d, c, dts, p, start = case
+    p.simulate(start, 0.8)
+    g64 = p.gradient()
+    J64 = float(p.loss())
+    q = GaugeMisfit(c, d["gauge_rows"], d["gauge_cols"], NSTEPS, dts, EVERY, K,
+                    obs=p.obs.cpu(), device=cuda, forward_dtype=torch.float32)
+    q.simulate(start, 0.8)
+    g32 = q.gradient()
+    J32 = float(q.loss())
+    rel = float(np.abs(g32 - g64).max() / np.abs(g64).max())
+    print(f"FP32-forward gradient vs FP64 adjoint: max rel diff {rel:.3e}; "
+          f"loss {J32:.6e} vs {J64:.6e}")
+    assert np.all(np.isfinite(g32))
+    assert abs(J32 - J64) <= 1e-3 * abs(J64)
+    assert rel <= 1e-3
