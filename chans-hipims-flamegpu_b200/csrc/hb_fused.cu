@@ -1767,18 +1767,23 @@ classify_tiles_kernel(const hb_instance *__restrict__ insts, const int32_t *__re
   // raster row y is code row y + HB_PAD_Y, raster column x code column
   // x + HB_CODE_PAD_X; the region lies inside the padded code array
   constexpr int W = TW + 8;
+  bool own = false;  // a valid cell among the tile's own cells
   for (int k = threadIdx.x; k < (TY + 4) * W; k += kRowsNT) {
     const int y = y0 - 2 + k / W, x = x0 - 4 + k % W;
     const uint8_t c = in.code[(size_t)(y + HB_PAD_Y) * in.code_pitch + (x + HB_CODE_PAD_X)];
     ok = ok && is_valid(c);
+    own = own || (is_valid(c) && y >= y0 && y < y0 + TY && x >= x0 && x < x0 + TW);
   }
   ok = __syncthreads_and(ok) != 0;
-  if (threadIdx.x == 0) flags[tile] = ok ? 1 : 0;
+  own = __syncthreads_or(own) != 0;
+  // 2 (64-wide tiles only): no valid cell of its own, nothing to step
+  if (threadIdx.x == 0) flags[tile] = ok ? 1 : ((TW == kPW && !own) ? 2 : 0);
 }
 
 // Stable partition of the tiles by flag, one block: order = general tiles
-// (flag 0) in index order, then all-valid tiles (flag 1) in index order;
-// counts = {general, all-valid}.
+// (flags 0 and 2) in index order, then all-valid tiles (flag 1) in index
+// order; counts = {general, all-valid}.  A flag-2 tile (no valid cell) is
+// listed as ~tile.
 constexpr int kOrderNT = 1024;
 __global__ void __launch_bounds__(kOrderNT)
 order_tiles_kernel(const uint8_t *__restrict__ flags, int n, int32_t *__restrict__ order,
@@ -1789,7 +1794,7 @@ order_tiles_kernel(const uint8_t *__restrict__ flags, int n, int32_t *__restrict
   if (tid == 0) s_total = 0;
   __syncthreads();
   int cnt = 0;
-  for (int i = tid; i < n; i += kOrderNT) cnt += flags[i] == 0;
+  for (int i = tid; i < n; i += kOrderNT) cnt += flags[i] != 1;
   atomicAdd(&s_total, cnt);
   __syncthreads();
   if (tid == 0) {
@@ -1800,8 +1805,8 @@ order_tiles_kernel(const uint8_t *__restrict__ flags, int n, int32_t *__restrict
   const unsigned below = (1u << lane) - 1u;
   for (int c = 0; c < n; c += kOrderNT) {
     const int i = c + tid;
-    const int f = i < n ? flags[i] : 2;
-    const unsigned bg = __ballot_sync(0xffffffffu, f == 0);
+    const int f = i < n ? flags[i] : 3;  // past the end: in neither list
+    const unsigned bg = __ballot_sync(0xffffffffu, f == 0 || f == 2);
     const unsigned ba = __ballot_sync(0xffffffffu, f == 1);
     if (lane == 0) {
       s_g[w] = __popc(bg);
@@ -1813,7 +1818,7 @@ order_tiles_kernel(const uint8_t *__restrict__ flags, int n, int32_t *__restrict
       og += s_g[q];
       oa += s_a[q];
     }
-    if (f == 0) order[s_base[0] + og + __popc(bg & below)] = i;
+    if (f == 0 || f == 2) order[s_base[0] + og + __popc(bg & below)] = f == 2 ? ~i : i;
     if (f == 1) order[s_base[1] + oa + __popc(ba & below)] = i;
     __syncthreads();
     if (tid == 0) {

@@ -351,6 +351,7 @@ struct PairSmem {
   int red_i[kRowsNW];
   int last;
   int last2;
+  unsigned rowmask;           // general tiles: bit i set if row i holds a valid cell
   static constexpr unsigned kTxBytes =
       (unsigned)(4 * SH * kPSWF * sizeof(float) + TY * kPW * sizeof(float) + SH * kPSWC);
 };
@@ -477,8 +478,11 @@ __device__ __forceinline__ Fc2 face_pair(const PairSmem<TY> &s, const Cel2 &A, c
 // Returns false when the tile's data did not arrive within the bounded wait
 // (the instance's status says so; the caller leaves).
 // ===========================================================================
+// empty (general build only): the tile holds no valid cell (prepare found it
+// so); it loads nothing and adds a zero partial to its group.
 template <int TY, bool SOURCES, int PATH>
 __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, const int tile,
+                                          const bool empty,
                                           const hb_instance *__restrict__ insts,
                                           const int32_t *__restrict__ tile_inst,
                                           TilePartial *__restrict__ partials,
@@ -487,6 +491,7 @@ __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, cons
                                           const CUtensorMap *__restrict__ maps) {
   constexpr bool kAllValid = PATH == 1;
   constexpr bool ALLV = kAllValid;
+  const bool skip = !kAllValid && empty;
   using S = PairSmem<TY>;
   constexpr int R = S::R;
   const PairView<TY> V{s};
@@ -509,7 +514,7 @@ __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, cons
   const int P = in.pitch;
   const CUtensorMap *m = maps + (size_t)ii * kMapsPerInstance;
 
-  if (tid == 0) {
+  if (tid == 0 && !skip) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(&s.bar, S::kTxBytes);
     tma_load_2d(s.f[0], m + 0 + cur, x0, y0, &s.bar);
@@ -529,7 +534,7 @@ __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, cons
   }
   const int bug_y = in.bug_y, bug_x = in.bug_x;
   float datum_tile = 0.f;
-  if (in.datum) {
+  if (in.datum && !skip) {
     const int by = y0 / HB_DATUM_BLOCK, bx = x0 / HB_DATUM_BLOCK;
     datum_tile = in.datum[by * in.datum_nx + bx];
     if (tid >= 32 && tid < 41) {
@@ -539,14 +544,31 @@ __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, cons
       s.ddatum[q] = in.datum[yy * in.datum_nx + xx] - datum_tile;
     }
   }
-  const bool arrived = mbar_wait(&s.bar, phase, 4000000000LL);
-  if (__syncthreads_or(!arrived)) {
-    if (tid == 0) atomicOr(&ctrl->status, 2);
-    mbar_wait(&s.bar, phase, 4000000000LL);
-    return false;
+  if (!skip) {
+    const bool arrived = mbar_wait(&s.bar, phase, 4000000000LL);
+    if (__syncthreads_or(!arrived)) {
+      if (tid == 0) atomicOr(&ctrl->status, 2);
+      mbar_wait(&s.bar, phase, 4000000000LL);
+      return false;
+    }
+    phase ^= 1u;
   }
-  phase ^= 1u;
-  if (in.datum) {
+  if constexpr (!ALLV) {
+    // rows of the tile that hold a valid cell (lane i: row i, 16 words of 4
+    // codes; a code is valid unless its class nibble is the no-data class)
+    if (w == 0) {
+      bool rv = false;
+      if (!skip && lane < TY) {
+        const uint32_t *row = reinterpret_cast<const uint32_t *>(&s.code[(lane + 2) * kPSWC + 16]);
+#pragma unroll
+        for (int q = 0; q < kPW / 4; ++q)
+          rv = rv || (row[q] & 0xF0F0F0F0u) != 0xF0F0F0F0u;
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, rv);
+      if (lane == 0) s.rowmask = m;
+    }
+  }
+  if (in.datum && !skip) {
     __syncthreads();  // ddatum visible
     const int by0 = (y0 / HB_DATUM_BLOCK) * HB_DATUM_BLOCK;
     const int bx0 = (x0 / HB_DATUM_BLOCK) * HB_DATUM_BLOCK;
@@ -566,7 +588,8 @@ __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, cons
   // --- tile edges: warp 0 the faces between columns 63 | 64 (east faces of
   // lane 31's second cell), two rows per lane; warp 1 the x-slopes of
   // column -1 (west neighbour of lane 0's first cell)
-  if (w == 0) {
+  if (skip) {
+  } else if (w == 0) {
     for (int i = 2 * lane; i < TY; i += 64) {
       float a[4], b[4];  // slopes of col 63 / col 64 for rows i, i + 1 (h, z, qx, qy)
       float a1[4], b1[4];
@@ -594,7 +617,17 @@ __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, cons
     }
   }
 
-  const int r0 = w * R;
+  // rows walked by this warp: all-valid tiles R rows each; general tiles
+  // share the rows from the first to the last one that holds a valid cell
+  // evenly among the warps (a tile over the catchment's edge with a few live
+  // rows then takes a few rows' time), none when the tile is empty
+  int r0 = w * R, r_end = r0 + R;
+  if constexpr (!ALLV) {
+    const unsigned m = s.rowmask;  // written before the barrier above
+    const int lo = m ? __ffs(m) - 1 : 0, hi = m ? 32 - __clz(m) : 0;
+    r0 = lo + (w * (hi - lo)) / kRowsNW;
+    r_end = lo + ((w + 1) * (hi - lo)) / kRowsNW;
+  }
   const int j0 = 2 * lane;  // this lane's first column
   const int rx0 = x0 + j0;
   f2 vol2 = dup(0.f);
@@ -641,7 +674,7 @@ __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, cons
     const float dtg = dt * kGF;
 
 #pragma unroll 1
-    for (int i = r0; i < r0 + R; ++i) {
+    for (int i = r0; i < r_end; ++i) {
       // --- x-direction: neighbours W (col 2j-1) and E (col 2j+2)
       const int kc = V.fi(i, j0);
       float Wv[4], Ev[4];
@@ -971,10 +1004,12 @@ pairs_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restri
   unsigned phase = 0;
   const int n_list = counts[PATH];
   const int32_t *list = order + (PATH == 1 ? counts[0] : 0);
-  for (int k = blockIdx.x; k < n_list; k += gridDim.x)
-    if (!pair_tile<TY, SOURCES, PATH>(s, phase, list[k], insts, tile_inst, partials, gparts,
-                                      gcount, bct, maps))
+  for (int k = blockIdx.x; k < n_list; k += gridDim.x) {
+    const int e = list[k];  // ~tile: a general tile without valid cells
+    if (!pair_tile<TY, SOURCES, PATH>(s, phase, e < 0 ? ~e : e, e < 0, insts, tile_inst, partials,
+                                      gparts, gcount, bct, maps))
       return;
+  }
 }
 
 // ===========================================================================
@@ -998,6 +1033,7 @@ constexpr int kPersistMinBlocks = 4;
 // its own build (the general path's ghost faces would otherwise cost it spills).
 template <int TY, bool SOURCES>
 __device__ __noinline__ bool pair_tile_general(PairSmem<TY> &s, unsigned &phase, const int tile,
+                                               const bool empty,
                                                const hb_instance *__restrict__ insts,
                                                const int32_t *__restrict__ tile_inst,
                                                TilePartial *__restrict__ partials,
@@ -1005,8 +1041,8 @@ __device__ __noinline__ bool pair_tile_general(PairSmem<TY> &s, unsigned &phase,
                                                unsigned *__restrict__ gcount,
                                                BcTable *__restrict__ bct,
                                                const CUtensorMap *__restrict__ maps) {
-  return pair_tile<TY, SOURCES, 0>(s, phase, tile, insts, tile_inst, partials, gparts, gcount, bct,
-                                   maps);
+  return pair_tile<TY, SOURCES, 0>(s, phase, tile, empty, insts, tile_inst, partials, gparts,
+                                   gcount, bct, maps);
 }
 
 template <int TY, bool SOURCES>
@@ -1043,11 +1079,12 @@ pairs_persistent_kernel(const hb_instance *__restrict__ insts,
       const unsigned long long k = s_tile;
       __syncthreads();
       if (k >= n) break;
-      const int tile = order[k];
-      const bool ok = allvalid[tile]
-                          ? pair_tile<TY, SOURCES, 1>(s, phase, tile, insts, tile_inst, partials,
-                                                      gparts, gcount, bct, maps)
-                          : pair_tile_general<TY, SOURCES>(s, phase, tile, insts, tile_inst,
+      const int e = order[k];  // ~tile: a general tile without valid cells
+      const int tile = e < 0 ? ~e : e;
+      const bool ok = allvalid[tile] == 1
+                          ? pair_tile<TY, SOURCES, 1>(s, phase, tile, false, insts, tile_inst,
+                                                      partials, gparts, gcount, bct, maps)
+                          : pair_tile_general<TY, SOURCES>(s, phase, tile, e < 0, insts, tile_inst,
                                                            partials, gparts, gcount, bct, maps);
       if (!ok) {
         if (tid == 0) gave_up.fetch_or(1ull, cuda::memory_order_relaxed);

@@ -107,7 +107,7 @@ class GaugeMisfit:
         # the reverse sweep reads the FP64 instance record (bed, codes, tables)
         # and FP64 states on the same dense layout
         self.fs64 = self.fs if forward_dtype == torch.float64 else FusedSolver(
-            self.catchment, dtype=torch.float64, device=device)
+            self.catchment, dtype=torch.float64, device=device, origin=self.fs.inst[0].origin)
         self.device = self.fs.device
         self.n_zones = len(catchment.manning)
         self.offsets = self.fs.cell_offsets(0, np.asarray(gauge_rows), np.asarray(gauge_cols))

@@ -77,10 +77,126 @@ def _round_up(x: int, m: int) -> int:
     return (x + m - 1) // m * m
 
 
-class _Instance:
-    """Device arrays of one catchment in the padded dense layout."""
+# Reach of a tile's stencil as the tile classification counts it: rows above
+# and below, columns left and right (the staged box of the step kernel).
+_REACH_Y, _REACH_X = 2, 4
 
-    def __init__(self, c: Catchment, dtype: torch.dtype, device, tile: tuple[int, int]):
+
+def tile_grid_cost(valid: np.ndarray, tile: tuple[int, int], origin: tuple[int, int],
+                   bug: tuple[int, int] | None = None) -> float:
+    """Modelled time of one step of the two-cells-per-lane kernel over
+    `valid` when `origin` = (rows, cols) of no-data are put above and left of
+    the raster, in units of an all-valid tile: a general tile costs
+    0.4 + 1.1 x (rows per warp) / (ty / 4), its four warps sharing the rows
+    from its first to its last row with a valid cell; a tile without valid
+    cells 0.1."""
+    valid = np.asarray(valid, dtype=bool)
+    S = _prefix(valid)
+    return float(_grid_cost(S, valid.shape, tile, np.array([origin[0]]), np.array([origin[1]]),
+                            bug)[0])
+
+
+def _prefix(valid: np.ndarray) -> np.ndarray:
+    rows, cols = valid.shape
+    S = np.zeros((rows + 1, cols + 1), dtype=np.int32)
+    S[1:, 1:] = np.cumsum(np.cumsum(valid, axis=0, dtype=np.int32), axis=1)
+    return S
+
+
+def _grid_cost(S, shape, tile, sy: np.ndarray, sx: np.ndarray, bug) -> np.ndarray:
+    """tile_grid_cost for origins (sy[k], sx[k]) at once (prefix sums S)."""
+    rows, cols = shape
+    ty, tx = tile
+
+    def count(y0, y1, x0, x1):  # valid cells in [y0, y1) x [x0, x1), clipped
+        y0, y1 = np.clip(y0, 0, rows), np.clip(y1, 0, rows)
+        x0, x1 = np.clip(x0, 0, cols), np.clip(x1, 0, cols)
+        return S[y1, x1] - S[y0, x1] - S[y1, x0] + S[y0, x0]
+
+    nty, ntx = (rows + sy + ty - 1) // ty, (cols + sx + tx - 1) // tx  # per origin
+    y0 = np.arange(nty.max())[None, :, None] * ty - sy[:, None, None]
+    x0 = np.arange(ntx.max())[None, None, :] * tx - sx[:, None, None]
+    exists = ((np.arange(nty.max())[None, :, None] < nty[:, None, None]) &
+              (np.arange(ntx.max())[None, None, :] < ntx[:, None, None]))
+    by0, by1 = y0 - _REACH_Y, y0 + ty + _REACH_Y
+    bx0, bx1 = x0 - _REACH_X, x0 + tx + _REACH_X
+    inside = (by0 >= 0) & (by1 <= rows) & (bx0 >= 0) & (bx1 <= cols)
+    allv = inside & (count(by0, by1, bx0, bx1) == (by1 - by0) * (bx1 - bx0))
+    if bug is not None and bug[0] >= 0:
+        allv &= ~((bug[0] >= by0) & (bug[0] < by1) & (bug[1] >= bx0) & (bug[1] < bx1))
+    cost = np.where(allv & exists, 1.0, 0.0)
+    g = np.nonzero(exists & ~allv)  # general tiles: rows from the first to the last live one
+    gy = np.broadcast_to(y0, allv.shape)[g][:, None] + np.arange(ty)[None, :]
+    gx = np.broadcast_to(x0, allv.shape)[g][:, None]
+    live = count(gy, gy + 1, gx, gx + tx) > 0
+    lo = np.where(live.any(-1), live.argmax(-1), 0)
+    hi = np.where(live.any(-1), ty - live[:, ::-1].argmax(-1), 0)
+    per_warp = -(-(hi - lo) // 4)  # rows of the warp that walks most
+    cost[g] = np.where(hi > lo, 0.4 + 1.1 * per_warp / (ty / 4), 0.1)
+    return cost.sum(axis=(1, 2))
+
+
+def tile_origin(valid: np.ndarray, tile: tuple[int, int],
+                bug: tuple[int, int] | None = None) -> tuple[int, int]:
+    """Rows and columns of no-data to put above and left of a catchment so
+    that its tile grid costs least under tile_grid_cost: the all-valid tiles
+    then start where the valid cells do, and the tiles over the catchment's
+    edges hold as few rows as they can.  Coordinate descent over the column
+    and row shifts (smallest shift among equals)."""
+    ty, tx = tile
+    valid = np.asarray(valid, dtype=bool)
+    if not valid.any():
+        return (0, 0)
+    S = _prefix(valid)
+    sy, sx = 0, 0
+
+    def best(cy, cx):
+        k = int(np.argmin(_grid_cost(S, valid.shape, tile, cy, cx, bug)))  # first minimum
+        return int(cy[k]), int(cx[k])
+
+    for axis in (1, 0, 1):
+        n = ty if axis == 0 else tx
+        sy, sx = best(np.arange(n) if axis == 0 else np.full(n, sy),
+                      np.arange(n) if axis == 1 else np.full(n, sx))
+    return (sy, sx)
+
+
+def _shift_catchment(c: Catchment, sy: int, sx: int) -> Catchment:
+    """c with sy rows and sx columns of no-data (zeros) above and left of
+    every raster field."""
+    if sy == 0 and sx == 0:
+        return c
+    pad = lambda a: None if a is None else np.pad(np.asarray(a), ((sy, 0), (sx, 0)))
+    return dataclasses.replace(
+        c, mask=pad(c.mask), z=pad(c.z), h=pad(c.h), qx=pad(c.qx), qy=pad(c.qy),
+        zone=pad(c.zone), h_max=pad(c.h_max), cum=pad(c.cum), rain_station=pad(c.rain_station))
+
+
+def _first_valid_cell(mask) -> tuple[int, int] | None:
+    """(row, col) of the first valid cell in row-major order (compacted
+    cell 0 of the reference), or None."""
+    m = np.asarray(mask)
+    flat = np.flatnonzero(m.ravel() > 0)
+    return None if flat.size == 0 else (int(flat[0] // m.shape[1]), int(flat[0] % m.shape[1]))
+
+
+class _Instance:
+    """Device arrays of one catchment in the padded dense layout.
+
+    origin = (sy, sx): the kernels see the catchment with sy rows and sx
+    columns of no-data above and left of it (the tile grid starts that far
+    before the raster).  `raster()` views and `valid` are in the catchment's
+    own coordinates; `rows`, `cols` and `bug` in the kernels' raster."""
+
+    def __init__(self, c: Catchment, dtype: torch.dtype, device, tile: tuple[int, int],
+                 origin: tuple[int, int] = (0, 0)):
+        sy, sx = (int(origin[0]), int(origin[1]))
+        if sy < 0 or sx < 0:
+            raise ValueError("the tile grid origin must be >= 0 in rows and columns")
+        self.origin = (sy, sx)
+        self.crows, self.ccols = np.asarray(c.mask).shape
+        c0 = c
+        c = _shift_catchment(c, sy, sx)
         rows, cols = c.mask.shape
         self.rows, self.cols = rows, cols
         self.dx = float(c.dx)
@@ -94,7 +210,7 @@ class _Instance:
         PY, PX, CPX = _lib.HB_PAD_Y, _lib.HB_PAD_X, _lib.HB_CODE_PAD_X
         mask = np.asarray(c.mask)
         valid = mask > 0
-        self.valid = valid
+        self.valid = valid[sy:, sx:]
         self.n_valid = int(valid.sum())
 
         # boundary classes: distinct type codes of valid cells
@@ -141,7 +257,7 @@ class _Instance:
         self.initial_h_max = self.h_max.clone()
         self.code = torch.as_tensor(code_np, device=device).contiguous()
         self.datum = torch.as_tensor(datum, dtype=torch.float32, device=device).contiguous()
-        self.z_abs_offset = dfull
+        self.z_abs_offset = dfull[sy:, sx:]
 
         def table(a, width):
             if a is None:
@@ -194,11 +310,12 @@ class _Instance:
             self.bc_type[k] = bt
             self.bc_id[k] = bid
         self.manning = list(c.manning) + [0.0] * (_lib.HB_MAX_ZONES - len(c.manning))
-        self.catchment = c
+        self.catchment = c0
 
     def raster(self, t: torch.Tensor) -> torch.Tensor:
-        PY, PX = _lib.HB_PAD_Y, _lib.HB_PAD_X
-        return t[PY:PY + self.rows, PX:PX + self.cols]
+        """The catchment's rows x cols view of a dense array."""
+        PY, PX = _lib.HB_PAD_Y + self.origin[0], _lib.HB_PAD_X + self.origin[1]
+        return t[PY:PY + self.crows, PX:PX + self.ccols]
 
 
 class FusedSolver:
@@ -210,12 +327,19 @@ class FusedSolver:
 
     tile = (rows, cols): (32, 64) runs two cells per lane (FP32 2nd order, the
     default there); (32, 32) and (64, 32) one cell per lane (every dtype and
-    order)."""
+    order).
+
+    origin: rows and columns of no-data the kernels see above and left of each
+    catchment, i.e. where the tile grid starts (results are given back in the
+    catchment's own coordinates).  None: chosen per catchment by tile_origin
+    for 32 x 64 tiles, (0, 0) for the others; a pair: every catchment; a list:
+    one pair per catchment.  In FP32 the bed datum blocks move with the grid,
+    so runs on different origins differ by round-off."""
 
     def __init__(self, catchments: Catchment | Sequence[Catchment], dtype=torch.float32,
                  tile: tuple[int, int] | None = None, device="cuda", grid_blocks: int = 0,
                  exact_fp32: bool = False, kernel: str = "rows", minb: int = 0,
-                 order: int = 2):
+                 order: int = 2, origin=None):
         if isinstance(catchments, Catchment):
             catchments = [catchments]
         if dtype not in (torch.float32, torch.float64):
@@ -233,7 +357,17 @@ class FusedSolver:
             pairs = dtype == torch.float32 and kernel == "rows" and order == 2 and not exact_fp32
             tile = (32, 64) if pairs else (32, 32)
         self.tile = tuple(tile)
-        self.inst = [_Instance(c, dtype, self.device, self.tile) for c in catchments]
+        if origin is None:
+            origins = [tile_origin(np.asarray(c.mask) > 0, self.tile, _first_valid_cell(c.mask))
+                       if self.tile == (32, 64) else (0, 0) for c in catchments]
+        elif len(origin) == 2 and np.isscalar(origin[0]):
+            origins = [tuple(origin)] * len(catchments)
+        else:
+            origins = [tuple(o) for o in origin]
+            if len(origins) != len(catchments):
+                raise ValueError("origin: one (rows, cols) pair per catchment")
+        self.inst = [_Instance(c, dtype, self.device, self.tile, o)
+                     for c, o in zip(catchments, origins)]
         n = len(self.inst)
         self._ctrl_size = ctypes.sizeof(_lib.HbCtrl)
         ctrl_host = (_lib.HbCtrl * n)()
@@ -598,7 +732,9 @@ class FusedSolver:
     def cell_offsets(self, k: int, rows: np.ndarray, cols: np.ndarray) -> torch.Tensor:
         """Flat element offsets of raster cells in the dense state arrays (for gather)."""
         ins = self.inst[k]
-        off = (np.asarray(rows) + _lib.HB_PAD_Y) * ins.pitch + (np.asarray(cols) + _lib.HB_PAD_X)
+        sy, sx = ins.origin
+        off = ((np.asarray(rows) + _lib.HB_PAD_Y + sy) * ins.pitch +
+               (np.asarray(cols) + _lib.HB_PAD_X + sx))
         return torch.as_tensor(off.astype(np.int64), device=self.device)
 
     def current(self, k: int = 0) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor]:

@@ -117,6 +117,16 @@ def _static_halos(fs: FusedSolver, k: int, c: Catchment, a: int, b: int) -> None
             ins.z[pr].copy_(torch.as_tensor(zrow, dtype=fs.dtype, device=fs.device))
 
 
+def _unshifted(solver_kw: dict) -> dict:
+    """Strips keep the tile grid at the raster's origin: their halo rows,
+    datum blocks and strip edges are laid out on it."""
+    kw = dict(solver_kw)
+    if tuple(kw.get("origin") or (0, 0)) != (0, 0):
+        raise ValueError("strips run with the tile grid at the raster origin")
+    kw["origin"] = (0, 0)
+    return kw
+
+
 def _state_arrays(ins) -> list[torch.Tensor]:
     """[h0, h1, qx0, qx1, qy0, qy1] of one instance (the halo_* order)."""
     return [ins.h[0], ins.h[1], ins.qx[0], ins.qx[1], ins.qy[0], ins.qy[1]]
@@ -149,7 +159,7 @@ class StripSolver:
         self.ranges = split_rows(mask.shape[0], parts)
         self.catchment = c
         strips = [strip_catchment(c, a, b) for a, b in self.ranges]
-        self.fs = FusedSolver(strips, dtype=dtype, device=device, **solver_kw)
+        self.fs = FusedSolver(strips, dtype=dtype, device=device, **_unshifted(solver_kw))
         self.device = self.fs.device
         gbug = _first_valid(mask)
         for k, (a, b) in enumerate(self.ranges):
@@ -220,7 +230,8 @@ class DistributedStrips:
         self.rank, self.world = rank, world
         self.ranges = split_rows(mask.shape[0], world)
         a, b = self.ranges[rank]
-        self.fs = FusedSolver(strip_catchment(c, a, b), dtype=dtype, device=device, **solver_kw)
+        self.fs = FusedSolver(strip_catchment(c, a, b), dtype=dtype, device=device,
+                              **_unshifted(solver_kw))
         self.device = self.fs.device
         _static_halos(self.fs, 0, c, a, b)
         gbug = _first_valid(mask)

@@ -100,3 +100,93 @@ def test_rain_interpolation_matches_oracle_cursor():
     for t, want in ((0.0, [1.0, 2.0]), (5.0, [2.0, 1.0]), (20.0, [1.5, 0.5]), (30.0, [0, 0])):
         g.t = torch.tensor([t], dtype=torch.float64)
         np.testing.assert_allclose(g._interp_rain(R), want)
+
+
+def _brute_grid_cost(valid, tile, origin, bug):
+    """tile_grid_cost restated tile by tile."""
+    ty, tx = tile
+    sy, sx = origin
+    rows, cols = valid.shape
+    pv = np.zeros((rows + sy + ty + 8, cols + sx + tx + 16), dtype=bool)
+    pv[4 + sy:4 + sy + rows, 8 + sx:8 + sx + cols] = valid  # kernel raster at (4, 8)
+    kb = None if bug is None else (bug[0] + sy, bug[1] + sx)
+    total = 0.0
+    for a in range((rows + sy + ty - 1) // ty):
+        for b in range((cols + sx + tx - 1) // tx):
+            y0, x0 = a * ty, b * tx
+            box = pv[4 + y0 - 2:4 + y0 + ty + 2, 8 + x0 - 4:8 + x0 + tx + 4]
+            allv = box.all() and not (kb is not None and y0 - 2 <= kb[0] < y0 + ty + 2
+                                      and x0 - 4 <= kb[1] < x0 + tx + 4)
+            live = [i for i in range(ty) if pv[4 + y0 + i, 8 + x0:8 + x0 + tx].any()]
+            if allv:
+                total += 1.0
+            elif not live:
+                total += 0.1
+            else:
+                span = live[-1] + 1 - live[0]
+                total += 0.4 + 1.1 * (-(-span // 4)) / (ty / 4)
+    return total
+
+
+def test_tile_grid_cost_matches_tile_by_tile_count():
+    from hipims_b200.fused import _first_valid_cell, tile_grid_cost
+
+    rng = np.random.default_rng(3)
+    for n, m in ((130, 150), (97, 200)):
+        nodata = np.zeros((n, m), dtype=bool)
+        nodata[0, :] = nodata[-1, :] = nodata[:, 0] = nodata[:, -1] = True
+        nodata |= rng.uniform(size=(n, m)) < 0.002
+        mask = T.boundary_codes(nodata, default_bc=50)
+        valid = mask > 0
+        bug = _first_valid_cell(mask)
+        for origin in ((0, 0), (7, 63), (3, 17), (31, 1)):
+            assert tile_grid_cost(valid, (32, 64), origin, bug) == \
+                pytest.approx(_brute_grid_cost(valid, (32, 64), origin, bug), rel=1e-12), origin
+
+
+def test_tile_origin_on_a_ringed_square():
+    """A 2048 x 2048 catchment inside a one-cell no-data ring: the grid moves
+    so that 32 tile columns cover the valid columns exactly (two of them
+    general; the ring's columns fall in two tiles without valid cells), and
+    the tiles over the top and bottom edges hold few rows."""
+    from hipims_b200.fused import _first_valid_cell, tile_grid_cost, tile_origin
+
+    n = 2048
+    nodata = np.zeros((n + 2, n + 2), dtype=bool)
+    nodata[0, :] = nodata[-1, :] = nodata[:, 0] = nodata[:, -1] = True
+    mask = T.boundary_codes(nodata, default_bc=50)
+    valid = mask > 0
+    bug = _first_valid_cell(mask)
+    o = tile_origin(valid, (32, 64), bug)
+    assert o[1] == 63 and (n + 2 + o[0]) % 32 != 0
+    assert tile_grid_cost(valid, (32, 64), o, bug) < 0.96 * tile_grid_cost(valid, (32, 64),
+                                                                             (0, 0), bug)
+
+
+def test_shifted_layout_views_and_offsets():
+    """An instance on a shifted grid: the raster views, validity, bed and
+    gather offsets are those of the catchment; the kernels' raster is larger
+    by the shift, with no-data codes in the added rows and columns."""
+    d = S.urban_catchment(100, seed=1, rain_mm_h=60.0)
+    rng = np.random.default_rng(0)
+    d["h"] = np.where(d["mask"] > 0, rng.uniform(0, 0.2, d["mask"].shape), 0.0)
+    c = S.catchment_from(d)
+    a = _Instance(c, torch.float32, "cpu", (32, 64))
+    b = _Instance(c, torch.float32, "cpu", (32, 64), origin=(5, 11))
+    assert (b.rows, b.cols) == (a.rows + 5, a.cols + 11)
+    assert b.bug == (a.bug[0] + 5, a.bug[1] + 11)
+    np.testing.assert_array_equal(b.valid, a.valid)
+    np.testing.assert_array_equal(b.raster(b.h[0]).numpy(), a.raster(a.h[0]).numpy())
+    zb = b.raster(b.z).double().numpy() + b.z_abs_offset
+    v = d["mask"] > 0
+    assert np.abs(zb[v] - d["z"][v]).max() < 1e-5
+    code = b.code.numpy()
+    PY, CPX = _lib.HB_PAD_Y, _lib.HB_CODE_PAD_X
+    assert (code[PY:PY + 5, CPX:CPX + b.cols] >> 4 == _lib.HB_NODATA_CLASS).all()
+    assert (code[PY:PY + b.rows, CPX:CPX + 11] >> 4 == _lib.HB_NODATA_CLASS).all()
+    rr, cc = np.nonzero(v)
+    sy, sx = b.origin
+    off = (rr + PY + sy) * b.pitch + (cc + _lib.HB_PAD_X + sx)
+    np.testing.assert_array_equal(b.h[0].numpy().ravel()[off], a.raster(a.h[0]).numpy()[v])
+    with pytest.raises(ValueError):
+        _Instance(c, torch.float32, "cpu", (32, 64), origin=(-1, 0))

@@ -101,7 +101,7 @@ def test_strips_reproduce_the_undivided_run(cuda, dtype, parts, forward):
 
     d = S.urban_catchment(192, dx=2.0, seed=8, rain_mm_h=120.0)
     c = S.catchment_from(d)
-    one = FusedSolver(c, dtype=dtype, device=cuda)
+    one = FusedSolver(c, dtype=dtype, device=cuda, origin=(0, 0))  # the strips' tile grid
     st = StripSolver(c, parts, dtype=dtype, device=cuda, forward_halos=forward)
     for _ in range(3):
         one.step(20)
@@ -166,7 +166,7 @@ def test_peer_strips_on_one_device_reproduce_the_undivided_run(cuda):
         p.join(timeout=120)
         assert p.exitcode == 0
     d = S.urban_catchment(160, dx=2.0, seed=11, rain_mm_h=120.0)
-    one = FusedSolver(S.catchment_from(d), dtype=torch.float32, device=cuda)
+    one = FusedSolver(S.catchment_from(d), dtype=torch.float32, device=cuda, origin=(0, 0))
     one.step(30)
     want = one.state(0)
     c1 = one.controls()[0]
