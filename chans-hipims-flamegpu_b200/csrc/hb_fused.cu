@@ -541,9 +541,10 @@ finish_kernel(const hb_instance *__restrict__ insts, BcTable *__restrict__ bct,
 // [n_groups] TilePartial (sums of groups of kGroupTiles tiles), [n_groups]
 // unsigned group counters, [n_tiles] int32 tile order (rows kernel: general
 // tiles, then all-valid tiles), [2] int32 counts of the two, [n_tiles] uint8
-// all-valid flags, [n_instances] BcTable, then
-// [n_instances][kMapsPerInstance] CUtensorMap.  Instance i's groups start at
-// tile_begin / kGroupTiles + i, which never overlaps instance i + 1's.
+// all-valid flags, 64-wide tiles only: [n_tiles] TileEntry in the order's
+// order, then [n_instances] BcTable, then [n_instances][kMapsPerInstance]
+// CUtensorMap.  Instance i's groups start at tile_begin / kGroupTiles + i,
+// which never overlaps instance i + 1's.
 inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 inline size_t ws_partials_bytes(int n_tiles) { return align256((size_t)n_tiles * sizeof(TilePartial)); }
 inline int ws_n_groups(const hb_fused_batch *b) {
@@ -559,8 +560,23 @@ inline size_t ws_counts_offset(const hb_fused_batch *b) {
   return ws_order_offset(b) + align256((size_t)b->n_tiles * sizeof(int32_t));
 }
 inline size_t ws_flags_offset(const hb_fused_batch *b) { return ws_counts_offset(b) + 256; }
-inline size_t ws_bct_offset(const hb_fused_batch *b) {
+// What a tile of the two-cells-per-lane step needs before it can issue its
+// tile loads, in one 16-byte record: the tile (~tile when it holds no valid
+// cell), its instance and that instance's control block.
+struct alignas(16) TileEntry {
+  int32_t tile;
+  int32_t inst;
+  hb_ctrl *ctrl;
+};
+static_assert(sizeof(TileEntry) == 16, "one 16-byte load per tile");
+inline size_t ws_entries_offset(const hb_fused_batch *b) {
   return ws_flags_offset(b) + align256((size_t)b->n_tiles);
+}
+inline size_t ws_entries_bytes(const hb_fused_batch *b) {
+  return b->tile_x == 64 ? align256((size_t)b->n_tiles * sizeof(TileEntry)) : 0;
+}
+inline size_t ws_bct_offset(const hb_fused_batch *b) {
+  return ws_entries_offset(b) + ws_entries_bytes(b);
 }
 inline size_t ws_maps_offset(const hb_fused_batch *b) {
   return align256(ws_bct_offset(b) + (size_t)b->n_instances * sizeof(BcTable));
@@ -1838,6 +1854,22 @@ order_tiles_kernel(const uint8_t *__restrict__ flags, int n, int32_t *__restrict
   }
 }
 
+// The order as TileEntry records (64-wide tiles): entries[k] for order[k].
+__global__ void __launch_bounds__(256)
+tile_entries_kernel(const int32_t *__restrict__ order, int n,
+                    const int32_t *__restrict__ tile_inst, const hb_instance *__restrict__ insts,
+                    TileEntry *__restrict__ entries) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int e = order[k];
+  const int ii = tile_inst[e < 0 ? ~e : e];
+  TileEntry r;
+  r.tile = e;
+  r.inst = ii;
+  r.ctrl = insts[ii].ctrl;
+  entries[k] = r;
+}
+
 // Per-device side stream (highest priority) and fork/join events for the
 // general-tile kernel, created by hb_fused_prepare (outside any capture) and
 // kept until exit.  The mutex keeps one fork/join sequence whole when several
@@ -1946,26 +1978,29 @@ int launch_pairs_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
     return set_error(HB_ERR_ARG, "hb_fused_step: run hb_fused_prepare on this device first");
   const SideRes &sr = g_side[dev];
   const int n = b->n_tiles;
-  int n_general = n;
+  // the list lengths come from prepare (one read-back there), so that a
+  // tile's first load is its own entry
   const auto it = g_general_tiles.find(b->workspace);
-  if (it != g_general_tiles.end()) n_general = std::max(it->second, 1);
-  const int grid_a = b->grid_blocks > 0 ? std::min(b->grid_blocks, n) : n;
-  const int grid_g = b->grid_blocks > 0 ? std::min(b->grid_blocks, n) : std::min(n_general, n);
+  if (it == g_general_tiles.end())
+    return set_error(HB_ERR_ARG, "hb_fused_step: run hb_fused_prepare on this workspace first");
+  const int n_general = std::min(std::max(it->second, 0), n), n_valid = n - n_general;
+  const int grid_a = std::max(b->grid_blocks > 0 ? std::min(b->grid_blocks, n_valid) : n_valid, 1);
+  const int grid_g = std::max(b->grid_blocks > 0 ? std::min(b->grid_blocks, n_general) : n_general,
+                              1);
   char *ws = reinterpret_cast<char *>(b->workspace);
   TilePartial *parts = reinterpret_cast<TilePartial *>(ws);
   TilePartial *gparts = reinterpret_cast<TilePartial *>(ws + ws_partials_bytes(b->n_tiles));
   unsigned *gcount = reinterpret_cast<unsigned *>(ws + ws_gcount_offset(b));
-  const int32_t *order = reinterpret_cast<const int32_t *>(ws + ws_order_offset(b));
-  const int32_t *counts = reinterpret_cast<const int32_t *>(ws + ws_counts_offset(b));
+  const TileEntry *entries = reinterpret_cast<const TileEntry *>(ws + ws_entries_offset(b));
   BcTable *bct = reinterpret_cast<BcTable *>(ws + ws_bct_offset(b));
   const CUtensorMap *maps = reinterpret_cast<const CUtensorMap *>(ws + ws_maps_offset(b));
   for (int k = 0; k < nsteps; k++) {
     cudaError_t e = cudaEventRecord(sr.fork, st);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(sr.stream, sr.fork, 0);
     if (e != cudaSuccess) return set_error(HB_ERR_CUDA, "hb_fused_step fork: %s", cudaGetErrorString(e));
-    kg<<<grid_g, kRowsNT, sizeof(S), sr.stream>>>(b->instances, b->tile_instance, order, counts,
-                                                  parts, gparts, gcount, bct, maps);
-    ka<<<grid_a, kRowsNT, sizeof(S), st>>>(b->instances, b->tile_instance, order, counts, parts,
+    kg<<<grid_g, kRowsNT, sizeof(S), sr.stream>>>(b->instances, entries, n_general, parts, gparts,
+                                                  gcount, bct, maps);
+    ka<<<grid_a, kRowsNT, sizeof(S), st>>>(b->instances, entries + n_general, n_valid, parts,
                                            gparts, gcount, bct, maps);
     e = cudaEventRecord(sr.join, sr.stream);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(st, sr.join, 0);
@@ -2156,6 +2191,10 @@ int prepare_impl(const hb_fused_batch *b, cudaStream_t st, CUtensorMap *host_map
     order_tiles_kernel<<<1, kOrderNT, 0, st>>>(
         flags, b->n_tiles, reinterpret_cast<int32_t *>(ws + ws_order_offset(b)),
         reinterpret_cast<int32_t *>(ws + ws_counts_offset(b)));
+    if (b->tile_x == kPW)
+      tile_entries_kernel<<<(b->n_tiles + 255) / 256, 256, 0, st>>>(
+          reinterpret_cast<const int32_t *>(ws + ws_order_offset(b)), b->n_tiles,
+          b->tile_instance, b->instances, reinterpret_cast<TileEntry *>(ws + ws_entries_offset(b)));
     int32_t counts[2] = {0, 0};
     cudaError_t e = cudaMemcpyAsync(counts, ws + ws_counts_offset(b), sizeof(counts),
                                     cudaMemcpyDeviceToHost, st);
@@ -2392,8 +2431,7 @@ int launch_persistent(const hb_fused_batch *b, int nsteps, long long budget, cud
   if (grid > b->n_tiles) grid = b->n_tiles;
   char *ws = reinterpret_cast<char *>(b->workspace);
   const hb_instance *insts = b->instances;
-  const int32_t *tile_inst = b->tile_instance;
-  const int32_t *order = reinterpret_cast<const int32_t *>(ws + ws_order_offset(b));
+  const TileEntry *entries = reinterpret_cast<const TileEntry *>(ws + ws_entries_offset(b));
   const int32_t *counts = reinterpret_cast<const int32_t *>(ws + ws_counts_offset(b));
   const uint8_t *allvalid = reinterpret_cast<const uint8_t *>(ws + ws_flags_offset(b));
   TilePartial *parts = reinterpret_cast<TilePartial *>(ws);
@@ -2405,8 +2443,7 @@ int launch_persistent(const hb_fused_batch *b, int nsteps, long long budget, cud
   int n_instances = b->n_instances;
   e = cudaMemsetAsync(sync, 0, 3 * sizeof(unsigned long long), st);
   if (e != cudaSuccess) return set_error(HB_ERR_CUDA, "hb_fused_run: %s", cudaGetErrorString(e));
-  void *args[] = {(void *)&insts, (void *)&tile_inst, (void *)&order, (void *)&counts,
-                  (void *)&allvalid, (void *)&parts, (void *)&gparts, (void *)&gcount,
+  void *args[] = {(void *)&insts, (void *)&entries, (void *)&counts, (void *)&allvalid, (void *)&parts, (void *)&gparts, (void *)&gcount,
                   (void *)&bct, (void *)&maps, (void *)&n_instances, (void *)&nsteps,
                   (void *)&sync, (void *)&budget};
   e = cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(kern), dim3(grid), dim3(kRowsNT),

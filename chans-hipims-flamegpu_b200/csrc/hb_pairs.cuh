@@ -478,27 +478,27 @@ __device__ __forceinline__ Fc2 face_pair(const PairSmem<TY> &s, const Cel2 &A, c
 // Returns false when the tile's data did not arrive within the bounded wait
 // (the instance's status says so; the caller leaves).
 // ===========================================================================
-// empty (general build only): the tile holds no valid cell (prepare found it
-// so); it loads nothing and adds a zero partial to its group.
+// One tile: en = its TileEntry (en.tile < 0: ~tile of a general tile that
+// holds no valid cell, which loads nothing and adds a zero partial to its
+// group).
 template <int TY, bool SOURCES, int PATH>
-__device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, const int tile,
-                                          const bool empty,
+__device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, const TileEntry en,
                                           const hb_instance *__restrict__ insts,
-                                          const int32_t *__restrict__ tile_inst,
                                           TilePartial *__restrict__ partials,
                                           TilePartial *__restrict__ gparts,
                                           unsigned *__restrict__ gcount, BcTable *__restrict__ bct,
                                           const CUtensorMap *__restrict__ maps) {
   constexpr bool kAllValid = PATH == 1;
   constexpr bool ALLV = kAllValid;
-  const bool skip = !kAllValid && empty;
+  const bool skip = !kAllValid && en.tile < 0;
+  const int tile = en.tile < 0 ? ~en.tile : en.tile;
   using S = PairSmem<TY>;
   constexpr int R = S::R;
   const PairView<TY> V{s};
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const int ii = tile_inst[tile];
+  const int ii = en.inst;
   const hb_instance &in = insts[ii];
-  hb_ctrl *ctrl = in.ctrl;
+  hb_ctrl *ctrl = en.ctrl;
   if (__ldcg(&ctrl->halted)) return true;
   const int lt = tile - in.tile_begin;
   const int tyi = lt / in.tiles_x, txi = lt - tyi * in.tiles_x;
@@ -988,9 +988,9 @@ __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, cons
 // default (a positive grid loops over the build's tiles).
 template <int TY, int MINB, bool SOURCES, int PATH>
 __global__ void __launch_bounds__(kRowsNT, MINB)
-pairs_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restrict__ tile_inst,
-                  const int32_t *__restrict__ order, const int32_t *__restrict__ counts,
-                  TilePartial *__restrict__ partials, TilePartial *__restrict__ gparts,
+pairs_step_kernel(const hb_instance *__restrict__ insts, const TileEntry *__restrict__ list,
+                  const int n_list, TilePartial *__restrict__ partials,
+                  TilePartial *__restrict__ gparts,
                   unsigned *__restrict__ gcount, BcTable *__restrict__ bct,
                   const CUtensorMap *__restrict__ maps) {
   using S = PairSmem<TY>;
@@ -1002,14 +1002,10 @@ pairs_step_kernel(const hb_instance *__restrict__ insts, const int32_t *__restri
   }
   __syncthreads();
   unsigned phase = 0;
-  const int n_list = counts[PATH];
-  const int32_t *list = order + (PATH == 1 ? counts[0] : 0);
-  for (int k = blockIdx.x; k < n_list; k += gridDim.x) {
-    const int e = list[k];  // ~tile: a general tile without valid cells
-    if (!pair_tile<TY, SOURCES, PATH>(s, phase, e < 0 ? ~e : e, e < 0, insts, tile_inst, partials,
-                                      gparts, gcount, bct, maps))
+  for (int k = blockIdx.x; k < n_list; k += gridDim.x)
+    if (!pair_tile<TY, SOURCES, PATH>(s, phase, list[k], insts, partials, gparts, gcount, bct,
+                                      maps))
       return;
-  }
 }
 
 // ===========================================================================
@@ -1032,23 +1028,21 @@ constexpr int kPersistMinBlocks = 4;
 // all-valid path inlined in the kernel gets the register allocation it gets in
 // its own build (the general path's ghost faces would otherwise cost it spills).
 template <int TY, bool SOURCES>
-__device__ __noinline__ bool pair_tile_general(PairSmem<TY> &s, unsigned &phase, const int tile,
-                                               const bool empty,
+__device__ __noinline__ bool pair_tile_general(PairSmem<TY> &s, unsigned &phase,
+                                               const TileEntry en,
                                                const hb_instance *__restrict__ insts,
-                                               const int32_t *__restrict__ tile_inst,
                                                TilePartial *__restrict__ partials,
                                                TilePartial *__restrict__ gparts,
                                                unsigned *__restrict__ gcount,
                                                BcTable *__restrict__ bct,
                                                const CUtensorMap *__restrict__ maps) {
-  return pair_tile<TY, SOURCES, 0>(s, phase, tile, empty, insts, tile_inst, partials, gparts,
-                                   gcount, bct, maps);
+  return pair_tile<TY, SOURCES, 0>(s, phase, en, insts, partials, gparts, gcount, bct, maps);
 }
 
 template <int TY, bool SOURCES>
 __global__ void __launch_bounds__(kRowsNT, kPersistMinBlocks)
 pairs_persistent_kernel(const hb_instance *__restrict__ insts,
-                        const int32_t *__restrict__ tile_inst, const int32_t *__restrict__ order,
+                        const TileEntry *__restrict__ entries,
                         const int32_t *__restrict__ counts, const uint8_t *__restrict__ allvalid,
                         TilePartial *__restrict__ partials, TilePartial *__restrict__ gparts,
                         unsigned *__restrict__ gcount, BcTable *__restrict__ bct,
@@ -1079,13 +1073,12 @@ pairs_persistent_kernel(const hb_instance *__restrict__ insts,
       const unsigned long long k = s_tile;
       __syncthreads();
       if (k >= n) break;
-      const int e = order[k];  // ~tile: a general tile without valid cells
-      const int tile = e < 0 ? ~e : e;
-      const bool ok = allvalid[tile] == 1
-                          ? pair_tile<TY, SOURCES, 1>(s, phase, tile, false, insts, tile_inst,
-                                                      partials, gparts, gcount, bct, maps)
-                          : pair_tile_general<TY, SOURCES>(s, phase, tile, e < 0, insts, tile_inst,
-                                                           partials, gparts, gcount, bct, maps);
+      const TileEntry en = entries[k];
+      const bool ok = en.tile >= 0 && allvalid[en.tile] == 1
+                          ? pair_tile<TY, SOURCES, 1>(s, phase, en, insts, partials, gparts,
+                                                      gcount, bct, maps)
+                          : pair_tile_general<TY, SOURCES>(s, phase, en, insts, partials, gparts,
+                                                           gcount, bct, maps);
       if (!ok) {
         if (tid == 0) gave_up.fetch_or(1ull, cuda::memory_order_relaxed);
         return;
