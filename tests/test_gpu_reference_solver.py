@@ -126,3 +126,56 @@ def test_reference_solver_equals_restated_solver(cuda, RefGodunov, order):
     for f in ("_h_internal", "_qx_internal", "_qy_internal", "_h_max"):
         np.testing.assert_allclose(getattr(a, f).cpu().numpy(), getattr(b, f).cpu().numpy(),
                                    rtol=0, atol=1e-12, err_msg=f)
+
+
+@pytest.mark.parametrize("size", [2, 3])
+def test_reference_parallel_solver_on_b200_modules(cuda, size):
+    """The reference's multi-GPU solver class, unmodified, with its ranks on
+    this library's drop-in modules and on the reference's own kernels built
+    for sm_100a: the same clock and fields on every rank, and rank strips
+    that meet in their overlap rows (1st order, the class's scheme: its
+    neighbour table has the 1st-order five rows)."""
+    from baseline import ref_gpu, ref_loop
+    from hipims_b200 import scenarios as S
+
+    if not ref_loop.available() or not ref_gpu.available():
+        pytest.skip("the reference solver or its sm_100a kernels are not staged")
+    d = S.urban_catchment(120, dx=2.0, seed=5, rain_mm_h=150.0)
+    # a 1 cm sheet everywhere (a rank without wet cells keeps its last time
+    # step, HP/Parallel_SWE_CUDA.py:492-494, which the MIN reduction then
+    # holds for all) and a pond that spreads across the strip edges
+    h0 = np.full(np.asarray(d["mask"]).shape, 0.01)
+    h0[20:50, 30:70] = 0.4
+    d["h"] = np.where(np.asarray(d["mask"]) > 0, h0, 0.0)
+    d["qx"] = np.zeros_like(d["h"])
+    d["qy"] = np.zeros_like(d["h"])
+    steps = 60
+    ours, splits = ref_loop.run_parallel_loop(
+        ref_loop.load_parallel_swe(ref_loop.b200_modules()).Parallel_SWE, d, cuda, steps, size)
+    theirs, _ = ref_loop.run_parallel_loop(
+        ref_loop.load_parallel_swe(ref_loop.reference_kernel_modules()).Parallel_SWE, d, cuda,
+        steps, size)
+    for a, b in zip(ours, theirs):
+        assert a.t.item() == pytest.approx(b.t.item(), rel=1e-12)
+        for f in ("_h_internal", "_qx_internal", "_qy_internal", "_h_max"):
+            np.testing.assert_allclose(getattr(a, f).cpu().numpy(), getattr(b, f).cpu().numpy(),
+                                       rtol=0, atol=1e-9, err_msg=f)
+    # the clock advanced well past the first steps, the pond's wave crossed a
+    # strip edge, and after the last exchange is received every cell held by
+    # two ranks has one value
+    assert ours[0].t.item() > 100 * d["first_dt"]
+    moving = [int((g._qy_internal.abs() > 1e-3).sum()) for g in ours]
+    assert sum(1 for m in moving if m > 0) >= 2, moving
+    mask = np.asarray(d["mask"])
+    seen = {}
+    for r, g in enumerate(ours):
+        g.update_overlap_receive()
+        a, b = ref_loop.rank_rows(splits, r, size, mask.shape[0])
+        rows, cols = np.nonzero(mask[a:b] > 0)
+        h = g._h_internal.cpu().numpy()
+        for k, (y, x) in enumerate(zip(rows + a, cols)):
+            if (y, x) in seen:
+                assert seen[(y, x)] == h[k], (r, y, x)
+            else:
+                seen[(y, x)] = h[k]
+    assert len(seen) == int((mask > 0).sum())
