@@ -275,11 +275,12 @@ def run_ours(args) -> None:
         # of the previous one (PCIe is full duplex)
         from hipims_b200.fused import HostStepper
 
-        hst = HostStepper(fs)
+        hst = HostStepper(fs, layout="compact")
         host_in = hst.in_buffers
-        e2e_path = ("HostStepper: pinned host h, qx, qy -> device; hb_fused_step; device -> "
-                    "pinned host, every step; inbound copy of step k+1 overlapping the "
-                    "outbound copy of step k")
+        e2e_path = ("HostStepper: pinned host h, qx, qy in the reference's compacted layout "
+                    "(valid cells, row-major) -> device, hb_state_layout into the dense "
+                    "arrays, hb_fused_step, hb_state_layout back -> pinned host, every step; "
+                    "inbound copy of step k+1 overlapping the outbound copy of step k")
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)

@@ -366,6 +366,25 @@ __global__ void gather_kernel(int64_t n, const int64_t *__restrict__ off,
   if (ov) ov[i] = wet ? qy[k] / hh : T(0);
 }
 
+// h, qx, qy between the dense arrays and compacted arrays (cell i at dense
+// offset off[i]); TO_DENSE: scatter, else gather.
+template <typename T, bool TO_DENSE>
+__global__ void state_layout_kernel(int64_t n, const int64_t *__restrict__ off, T *h, T *qx,
+                                    T *qy, T *ch, T *cqx, T *cqy) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t k = off[i];
+  if constexpr (TO_DENSE) {
+    h[k] = ch[i];
+    qx[k] = cqx[i];
+    qy[k] = cqy[i];
+  } else {
+    ch[i] = h[k];
+    cqx[i] = qx[k];
+    cqy[i] = qy[k];
+  }
+}
+
 bool bad_dtype(int dtype) { return dtype != HB_F32 && dtype != HB_F64; }
 
 }  // namespace
@@ -577,4 +596,31 @@ extern "C" int hb_gather(int dtype, int64_t n, const int64_t *cell_offsets, cons
         n, cell_offsets, (const float *)h, (const float *)qx, (const float *)qy,
         (float *)out_h, (float *)out_u, (float *)out_v);
   return check_launch("hb_gather");
+}
+
+extern "C" int hb_state_layout(int dtype, int64_t n, const int64_t *offsets, int to_dense,
+                               void *h, void *qx, void *qy, void *ch, void *cqx, void *cqy,
+                               void *stream) {
+  HB_REQUIRE(!bad_dtype(dtype), "hb_state_layout: bad dtype %d", dtype);
+  HB_REQUIRE(n >= 0, "hb_state_layout: negative n");
+  if (n == 0) return HB_OK;
+  HB_REQUIRE(offsets && h && qx && qy && ch && cqx && cqy, "hb_state_layout: null pointer");
+  auto s = as_stream(stream);
+  const unsigned nb = blocks_for(n, kThreads);
+  if (dtype == HB_F64) {
+    auto *a = (double *)h, *b = (double *)qx, *c = (double *)qy;
+    auto *d = (double *)ch, *e = (double *)cqx, *f = (double *)cqy;
+    if (to_dense)
+      state_layout_kernel<double, true><<<nb, kThreads, 0, s>>>(n, offsets, a, b, c, d, e, f);
+    else
+      state_layout_kernel<double, false><<<nb, kThreads, 0, s>>>(n, offsets, a, b, c, d, e, f);
+  } else {
+    auto *a = (float *)h, *b = (float *)qx, *c = (float *)qy;
+    auto *d = (float *)ch, *e = (float *)cqx, *f = (float *)cqy;
+    if (to_dense)
+      state_layout_kernel<float, true><<<nb, kThreads, 0, s>>>(n, offsets, a, b, c, d, e, f);
+    else
+      state_layout_kernel<float, false><<<nb, kThreads, 0, s>>>(n, offsets, a, b, c, d, e, f);
+  }
+  return check_launch("hb_state_layout");
 }

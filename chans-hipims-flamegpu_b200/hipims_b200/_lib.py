@@ -121,6 +121,7 @@ SIGNATURES = {
     "hb_adjoint_step": (_I, [_P, _P]),
     "hb_adjoint_gauge": (_I, [_L, _P, _P, _P, _P, ctypes.c_double, _P]),
     "hb_gather": (_I, [_I, _L, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "hb_state_layout": (_I, [_I, _L, _P, _I, _P, _P, _P, _P, _P, _P, _P]),
 }
 
 _lock = threading.Lock()

@@ -752,25 +752,33 @@ class HostStepper:
     reads one fixed device buffer per field (the control block's `cur` is set
     back to it before each step), so the inbound copy of step k+1 runs while
     the outbound copy of step k is still in flight: PCIe carries both
-    directions at once.  Ordering, by CUDA events on three streams:
-      * inbound copy k+1: after step k has read the input buffer;
-      * step k+1: after inbound copy k+1 and after outbound copy k has read the
-        output buffer;
-      * outbound copy k+1: after step k+1.
+    directions at once.
 
-    Buffers are pinned host tensors in the device's padded dense layout
-    (`in_buffers`, `out_buffers`: [h, qx, qy] per instance, in instance
-    order), so that every copy is one contiguous transfer: on the 2048^2 case,
-    pitched copies of the raster rows alone, which skip the 8 % of padding,
-    lowered the host-to-host step rate from 3.35 to 2.51 Gcell/s.
-    `raster(buf, k)` is the rows x cols view of instance k's cells in a
-    buffer.  Calls are asynchronous: `finish()` makes the caller's stream wait
-    for the last outbound copy, after which a synchronize makes `out_buffers`
-    valid.
+    layout "compact" (default): the host buffers hold the reference's own
+    layout, the valid cells of each instance in row-major order
+    (`in_buffers`, `out_buffers`: [h, qx, qy] per instance, views of one
+    pinned [3, n_valid] block each, so one copy per instance and direction);
+    hb_state_layout moves them between the copied device block and the dense
+    arrays of the step.  Ordering, by CUDA events on three streams:
+      * inbound copy k+1: after step k's scatter has read the device block;
+      * step k+1: after the inbound copy and its scatter;
+      * gather k+1 into the outbound device block: after outbound copy k has
+        read it; outbound copy k+1: after that gather.
+    layout "dense": the host buffers are the padded dense arrays themselves
+    (one contiguous copy per field; `raster(buf, k)` is the rows x cols view
+    of instance k's cells), the step waiting for the previous outbound copy.
+    On the 2048^2 case the dense arrays carry the padding and the tile grid's
+    leading no-data columns, about 10 % more bytes than the valid cells.
+
+    Calls are asynchronous: `finish()` makes the caller's stream wait for the
+    last outbound copy, after which a synchronize makes `out_buffers` valid.
     """
 
-    def __init__(self, fs: "FusedSolver"):
+    def __init__(self, fs: "FusedSolver", layout: str = "compact"):
+        if layout not in ("compact", "dense"):
+            raise ValueError("layout must be 'compact' or 'dense'")
         self.fs = fs
+        self.layout = layout
         dev = fs.device
         cs = fs.controls()
         self.read = cs[0].cur
@@ -778,27 +786,96 @@ class HostStepper:
             raise ValueError("HostStepper: every instance must read the same buffer index")
         fields = lambda b: [x for ins in fs.inst for x in (ins.h[b], ins.qx[b], ins.qy[b])]
         self._dev_in, self._dev_out = fields(self.read), fields(1 - self.read)
-        self.in_buffers = [torch.empty(x.shape, dtype=x.dtype).pin_memory() for x in self._dev_in]
-        self.out_buffers = [torch.empty(x.shape, dtype=x.dtype).pin_memory() for x in self._dev_in]
-        for hb, x in zip(self.in_buffers, self._dev_in):
-            hb.copy_(x)
+        if layout == "dense":
+            self.in_buffers = [torch.empty(x.shape, dtype=x.dtype).pin_memory()
+                               for x in self._dev_in]
+            self.out_buffers = [torch.empty(x.shape, dtype=x.dtype).pin_memory()
+                                for x in self._dev_in]
+            for hb, x in zip(self.in_buffers, self._dev_in):
+                hb.copy_(x)
+        else:
+            self._offsets, self._din, self._dout = [], [], []
+            self._in_blocks, self._out_blocks = [], []
+            for k, ins in enumerate(fs.inst):
+                r, c = np.nonzero(ins.valid)
+                self._offsets.append(fs.cell_offsets(k, r, c))
+                blk = lambda where: (torch.empty((3, r.size), dtype=fs.dtype, device=dev)
+                                     if where == "dev" else
+                                     torch.empty((3, r.size), dtype=fs.dtype).pin_memory())
+                self._din.append(blk("dev"))
+                self._dout.append(blk("dev"))
+                self._in_blocks.append(blk("host"))
+                self._out_blocks.append(blk("host"))
+            self.in_buffers = [b[j] for b in self._in_blocks for j in range(3)]
+            self.out_buffers = [b[j] for b in self._out_blocks for j in range(3)]
+            with torch.cuda.device(dev):
+                for k in range(len(fs.inst)):
+                    self._layout(k, self._dev_in, self._din[k], to_dense=False)
+                torch.cuda.current_stream(dev).synchronize()
+            for hb, db in zip(self._in_blocks, self._din):
+                hb.copy_(db)
         n = len(fs.inst)
         words = fs._ctrl_size // 4
         self._cur = fs.ctrl.view(torch.int32).view(n, words)[:, _lib.HbCtrl.cur.offset // 4]
         self._h2d = torch.cuda.Stream(dev)
         self._d2h = torch.cuda.Stream(dev)
         self._stepped = torch.cuda.Event()
+        self._expanded = torch.cuda.Event()
         self._copied_in = torch.cuda.Event()
         self._copied_out = torch.cuda.Event()
         self._any = False
 
+    def _layout(self, k: int, dense: list, block: torch.Tensor, to_dense: bool) -> None:
+        fs = self.fs
+        h, qx, qy = dense[3 * k:3 * k + 3]
+        off = self._offsets[k]
+        _lib.check(_lib.lib().hb_state_layout(
+            _lib.HB_F32 if fs.dtype == torch.float32 else _lib.HB_F64, off.numel(),
+            off.data_ptr(), 1 if to_dense else 0, h.data_ptr(), qx.data_ptr(), qy.data_ptr(),
+            block[0].data_ptr(), block[1].data_ptr(), block[2].data_ptr(),
+            torch.cuda.current_stream(fs.device).cuda_stream), "hb_state_layout")
+
     def raster(self, buf: torch.Tensor, k: int = 0) -> torch.Tensor:
-        """The rows x cols cells of instance k in one of its host buffers."""
+        """The rows x cols cells of instance k in one of its host buffers
+        (dense layout)."""
+        if self.layout != "dense":
+            raise ValueError("raster views need layout='dense'; compact buffers are the valid "
+                             "cells in row-major order")
         return self.fs.inst[k].raster(buf)
 
     def step(self) -> None:
         """Enqueue: copy in_buffers to the device, one fused step, copy the
         new state to out_buffers."""
+        if self.layout == "dense":
+            self._step_dense()
+            return
+        comp = torch.cuda.current_stream(self.fs.device)
+        if self._any:
+            self._h2d.wait_event(self._expanded)
+        with torch.cuda.stream(self._h2d):
+            for db, hb in zip(self._din, self._in_blocks):
+                db.copy_(hb, non_blocking=True)
+            self._copied_in.record(self._h2d)
+        comp.wait_event(self._copied_in)
+        with torch.cuda.device(self.fs.device):
+            for k in range(len(self.fs.inst)):
+                self._layout(k, self._dev_in, self._din[k], to_dense=True)
+            self._expanded.record(comp)
+            self._cur.fill_(self.read)
+            self.fs.step(1)
+            if self._any:
+                comp.wait_event(self._copied_out)
+            for k in range(len(self.fs.inst)):
+                self._layout(k, self._dev_out, self._dout[k], to_dense=False)
+        self._stepped.record(comp)
+        self._d2h.wait_event(self._stepped)
+        with torch.cuda.stream(self._d2h):
+            for hb, db in zip(self._out_blocks, self._dout):
+                hb.copy_(db, non_blocking=True)
+            self._copied_out.record(self._d2h)
+        self._any = True
+
+    def _step_dense(self) -> None:
         comp = torch.cuda.current_stream(self.fs.device)
         if self._any:
             self._h2d.wait_event(self._stepped)

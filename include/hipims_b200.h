@@ -169,8 +169,10 @@ int hb_fused_finish(const struct hb_fused_batch *batch, const double *ext, void 
  *    hb_fused_prepare does for a workspace), then runs nsteps steps; pass it
  *    on the first call and whenever the batch or its control blocks change.
  *  - Limits: hb_fused_workspace_size(b) <= 4 MiB (about 110,000 tiles, e.g.
- *    110 M cells with 32 x 32 tiles; about 100,000 with 256 instances) and at
- *    most 256 instances; larger batches get HB_ERR_LIMIT with a message.
+ *    110 M cells with 32 x 32 tiles; about 100,000 with 256 instances; with
+ *    64-wide tiles, which keep a 16-byte entry per tile, about 78,000, i.e.
+ *    160 M cells, and 70,000) and at most 256 instances; larger batches get
+ *    HB_ERR_LIMIT with a message.
  *  - Every call with prepare != 0 looks up the array's device address on the
  *    current device, and the first such call on a device creates the
  *    library's side stream and two events for that device (kept until exit;
@@ -236,6 +238,20 @@ int hb_adjoint_gauge(int64_t n, const int64_t *offsets, const double *h, const d
 int hb_gather(int dtype, int64_t n, const int64_t *cell_offsets, const void *h,
               const void *qx, const void *qy, void *out_h, void *out_u,
               void *out_v, void *stream);
+
+/* ======================================================================
+ * State layout (no reference counterpart: the reference holds h, qx, qy
+ * compacted, the valid cells in row-major order, h[mask > 0] of
+ * HP/SWE_CUDA.py:62-227).  Copies the three state fields between the dense
+ * arrays of the fused step and compacted arrays of n cells, cell i at dense
+ * element offset offsets[i] (row * pitch + col of the dense layout).
+ *   to_dense != 0: h[offsets[i]] = ch[i] (and qx, qy); 0: ch[i] = h[offsets[i]].
+ * Lets a host that keeps the reference's compacted state feed the fused step
+ * (a per-step host copy then moves n cells per field instead of the padded
+ * raster).
+ * ==================================================================== */
+int hb_state_layout(int dtype, int64_t n, const int64_t *offsets, int to_dense, void *h,
+                    void *qx, void *qy, void *ch, void *cqx, void *cqy, void *stream);
 
 #ifdef __cplusplus
 }

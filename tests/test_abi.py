@@ -67,6 +67,16 @@ def test_adjoint_rejects_bad_arguments():
     assert L.hb_adjoint_gauge(3, None, None, None, None, 1.0, None) == -1
 
 
+def test_state_layout_rejects_bad_arguments():
+    L = _lib.lib()
+    assert L.hb_state_layout(7, 4, None, 1, *([None] * 6), None) == -1
+    assert b"dtype" in L.hb_last_error()
+    assert L.hb_state_layout(1, -1, None, 1, *([None] * 6), None) == -1
+    assert L.hb_state_layout(1, 0, None, 1, *([None] * 6), None) == 0
+    assert L.hb_state_layout(1, 4, None, 0, *([None] * 6), None) == -1
+    assert b"null" in L.hb_last_error()
+
+
 def test_dropin_modules_have_reference_names():
     import euler_update
     import fluxCal_2ndOrder_jh_improved
@@ -106,17 +116,21 @@ def test_dropin_ops_check_inputs_like_the_reference():
 
 def test_noalloc_limit_matches_the_documented_tile_counts():
     """hb_fused_step_noalloc keeps its scratch in 4 MiB: the header's limits
-    (about 110,000 tiles, about 100,000 with 256 instances) hold for the
-    workspace size the library computes (pure host arithmetic)."""
+    (about 110,000 tiles, about 100,000 with 256 instances; 78,000 and 70,000
+    with 64-wide tiles) hold for the workspace size the library computes
+    (pure host arithmetic)."""
     L = _lib.lib()
 
-    def size(tiles, instances):
+    def size(tiles, instances, tile_x=32):
         b = _lib.HbFusedBatch()
-        b.n_tiles, b.n_instances = tiles, instances
+        b.n_tiles, b.n_instances, b.tile_x = tiles, instances, tile_x
         return L.hb_fused_workspace_size(ctypes.byref(b))
 
     mib4 = 4 << 20
     assert size(110_000, 1) <= mib4 < size(115_000, 1)
     assert size(100_000, 256) <= mib4 < size(105_000, 256)
+    # 64-wide tiles keep a 16-byte entry per tile: about 78,000 and 70,000
+    assert size(78_000, 1, 64) <= mib4 < size(80_000, 1, 64)
+    assert size(70_000, 256, 64) <= mib4 < size(72_000, 256, 64)
     # grows with tiles and instances (regions are 256-byte aligned, so by steps)
     assert size(1000, 1) < size(2000, 1) and size(1000, 1) < size(1000, 8)
