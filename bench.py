@@ -20,7 +20,9 @@ the time is the max over ranks and `value` counts the cells of all ranks.
 
 --impl reference times the reference's own HiPIMS kernels compiled for the
 host (oracle/_ref) under the reference's step order on this machine's CPU
-cores, on the same catchment.
+cores, on the same catchment: up to K full steps, stopping after 60 s of
+timed steps (the default K = 5000 would take about 13 minutes), so the run
+ends within a few minutes; `cpu_baseline.sample` names the steps timed.
 """
 from __future__ import annotations
 
@@ -137,9 +139,13 @@ def profiled_traffic() -> float | None:
         return None
 
 
-def cpu_reference_rate(d: dict, steps: int, warmup: int, threads: int | None = None) -> dict:
+def cpu_reference_rate(d: dict, steps: int, warmup: int, threads: int | None = None,
+                       budget_s: float = 60.0) -> dict:
     """Cells x steps / s of the reference's host-built kernels (or the
-    restatement when oracle/_ref is absent) on catchment d."""
+    restatement when oracle/_ref is absent) on catchment d: up to `steps`
+    full steps, stopping once `budget_s` seconds of timed steps have run (a
+    full 2048^2 step takes ~0.15 s on 16 host threads, so a default
+    5000-step request is a bounded sample of the same workload)."""
     from oracle import oracle as O
 
     kind = "reference" if O.ref_available() else "port"
@@ -147,13 +153,17 @@ def cpu_reference_rate(d: dict, steps: int, warmup: int, threads: int | None = N
     O.set_threads(threads)
     sim = O.Sim(d, order=2, backend="ref" if kind == "reference" else "oracle")
     sim.run(SPINUP + warmup)
-    t0 = time.perf_counter()
-    sim.run(steps)
-    el = time.perf_counter() - t0
-    return {"value": sim.N * steps / el / 1e9, "unit": METRIC, "cores": threads, "kind": kind,
-            "seconds": el, "steps": steps,
-            "sample": f"{steps} steps of the full {int(np.sqrt(sim.N))}^2 catchment after "
-                      f"{SPINUP + warmup} untimed steps, FP64, {threads} threads"}
+    done, el = 0, 0.0
+    while done < steps and el < budget_s:
+        t0 = time.perf_counter()
+        sim.run(1)
+        el += time.perf_counter() - t0
+        done += 1
+    return {"value": sim.N * done / el / 1e9, "unit": METRIC, "cores": threads, "kind": kind,
+            "seconds": el, "steps": done,
+            "sample": f"{done} steps of the full {int(np.sqrt(sim.N))}^2 catchment after "
+                      f"{SPINUP + warmup} untimed steps (at most {steps}, at most "
+                      f"{budget_s:.0f} s), FP64, {threads} threads"}
 
 
 def cpu_dam_break_rates(steps: int = 1000) -> dict:
@@ -184,7 +194,7 @@ def run_reference(args) -> None:
     cb = cpu_reference_rate(d, args.steps, args.warmup)
     line = {"metric": METRIC, "value": cb["value"], "unit": METRIC, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": cb["seconds"] / args.steps * 1e3, "higher_is_better": True,
+            "ms_per_step": cb["seconds"] / cb["steps"] * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference", "config": config_of(args.cells, 1),
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
@@ -403,7 +413,7 @@ def strip_config(args, world: int) -> dict:
 
 
 def plain_fp64_rate(d: dict, dev, steps: int = 50, reference_kernels: bool = True,
-                    order: int = 2) -> dict:
+                    order: int = 2, repeats: int = 3) -> dict:
     """The plain FP64 GPU path on the same catchment, wall clock per step: the
     reference's own solver class (HP/SWE_CUDA.py Godunov, unmodified, staged
     in baseline/_ref by baseline/install_ref_py.py) and its step loop
@@ -412,7 +422,10 @@ def plain_fp64_rate(d: dict, dev, steps: int = 50, reference_kernels: bool = Tru
     modules resolved to the reference's own kernels built for sm_100a
     (reference_kernels; baseline/build_ref_cuda.py) or to this library's
     drop-in modules.  Where the reference class is not staged, the restated
-    loop of hipims_b200.solver runs instead and `loop` says so."""
+    loop of hipims_b200.solver runs instead and `loop` says so.  The loop's
+    per-step allocator and host round trips make single timings noisy, so
+    `repeats` runs of `steps` steps are timed one after another and `value`
+    is their median (`runs` lists all)."""
     from baseline import ref_loop
 
     if reference_kernels:
@@ -455,18 +468,21 @@ def plain_fp64_rate(d: dict, dev, steps: int = 50, reference_kernels: bool = Tru
     import io
 
     # the reference's 1st-order addFlux prints t every step: kept, but not on stdout
+    n = int(g._h_internal.numel())
+    runs = []
     with contextlib.redirect_stdout(io.StringIO()):
         for _ in range(SPINUP):
             one()
         torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        for _ in range(steps):
-            one()
-        torch.cuda.synchronize(dev)
-        el = time.perf_counter() - t0
-    n = int(g._h_internal.numel())
-    return {"value": n * steps / el / 1e9, "unit": METRIC, "steps": steps, "dtype": "f64",
-            "loop": loop, "kernels": kernels, "path": f"{loop} on {kernels}, wall clock"}
+        for _ in range(repeats):
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                one()
+            torch.cuda.synchronize(dev)
+            runs.append(n * steps / (time.perf_counter() - t0) / 1e9)
+    return {"value": float(np.median(runs)), "unit": METRIC, "steps": steps, "repeats": repeats,
+            "runs": runs, "dtype": "f64", "loop": loop, "kernels": kernels,
+            "path": f"{loop} on {kernels}, wall clock, median of {repeats} runs"}
 
 
 def first_order_rates(d: dict, dev, args, flush: torch.Tensor, stream, steps: int = 500) -> dict:
@@ -563,16 +579,17 @@ def ensemble_rate(dev, steps: int, count: int = 64, seed: int = 0, plain_sample:
     picked = ds[:: max(count // plain_sample, 1)][:plain_sample]
     pl_cells, pl_s = 0, 0.0
     for d in picked:
-        r = plain_fp64_rate(d, dev, steps=5, reference_kernels=True)
+        r = plain_fp64_rate(d, dev, steps=20, reference_kernels=True)
         if not r.get("value"):
             plain = r
             break
         n = int(np.sum(np.asarray(d["mask"]) > 0))
-        pl_cells += n * 5
-        pl_s += n * 5 / (r["value"] * 1e9)
+        pl_cells += n * 20
+        pl_s += n * 20 / (r["value"] * 1e9)
     if plain is None and pl_s > 0:
         plain = {"value": pl_cells / pl_s / 1e9, "unit": METRIC, "catchments": len(picked),
-                 "steps_each": 5, "path": r["path"] + ", catchments one after another"}
+                 "steps_each": 20, "path": r["path"] + " per catchment, catchments one after "
+                                                      "another"}
     value = cells * steps / (ms_p * 1e-3) / 1e9
     peak, peak_kind = measured_peak()
     achieved = BYTES_PER_CELL_FP32 * cells * steps / (ms_p * 1e-3) / 1e9
