@@ -14,7 +14,7 @@ untimed warm-up steps, then K timed steps.  Each timed step is bracketed by
 CUDA events on the launching stream; a 256 MiB buffer is written between timed
 steps to flush the 126 MB L2.  nvidia-smi samples the SM clock every 200 ms
 from before the first timed step to after the last (the default K keeps the
-timed region above one second so that it holds several samples).  N > 1 (torchrun): every rank advances its own
+timed region near 0.6 s, four or more samples).  N > 1 (torchrun): every rank advances its own
 replica (weak scaling; the catchment does not shard without a halo exchange),
 the time is the max over ranks and `value` counts the cells of all ranks.
 
