@@ -758,12 +758,15 @@ class HostStepper:
     layout, the valid cells of each instance in row-major order
     (`in_buffers`, `out_buffers`: [h, qx, qy] per instance, views of one
     pinned [3, n_valid] block each, so one copy per instance and direction);
-    hb_state_layout moves them between the copied device block and the dense
-    arrays of the step.  Ordering, by CUDA events on three streams:
-      * inbound copy k+1: after step k's scatter has read the device block;
-      * step k+1: after the inbound copy and its scatter;
-      * gather k+1 into the outbound device block: after outbound copy k has
-        read it; outbound copy k+1: after that gather.
+    hb_state_layout moves them between the copied device blocks and the dense
+    arrays of the step.  The device blocks are double-buffered (step k uses
+    set k % 2), so consecutive copies in one direction follow each other
+    without waiting for the step.  Ordering, by CUDA events on three streams:
+      * inbound copy k: after the scatter of step k-2 has read its set;
+      * scatter k, step k: after inbound copy k (the step's dense input is
+        written by scatter k only after step k-1, in stream order);
+      * gather k into its outbound set: after outbound copy k-2 has read it;
+        outbound copy k: after that gather.
     layout "dense": the host buffers are the padded dense arrays themselves
     (one contiguous copy per field; `raster(buf, k)` is the rows x cols view
     of instance k's cells), the step waiting for the previous outbound copy.
@@ -794,7 +797,8 @@ class HostStepper:
             for hb, x in zip(self.in_buffers, self._dev_in):
                 hb.copy_(x)
         else:
-            self._offsets, self._din, self._dout = [], [], []
+            self._offsets = []
+            self._din, self._dout = ([], []), ([], [])  # two device sets each
             self._in_blocks, self._out_blocks = [], []
             for k, ins in enumerate(fs.inst):
                 r, c = np.nonzero(ins.valid)
@@ -802,17 +806,18 @@ class HostStepper:
                 blk = lambda where: (torch.empty((3, r.size), dtype=fs.dtype, device=dev)
                                      if where == "dev" else
                                      torch.empty((3, r.size), dtype=fs.dtype).pin_memory())
-                self._din.append(blk("dev"))
-                self._dout.append(blk("dev"))
+                for j in range(2):
+                    self._din[j].append(blk("dev"))
+                    self._dout[j].append(blk("dev"))
                 self._in_blocks.append(blk("host"))
                 self._out_blocks.append(blk("host"))
             self.in_buffers = [b[j] for b in self._in_blocks for j in range(3)]
             self.out_buffers = [b[j] for b in self._out_blocks for j in range(3)]
             with torch.cuda.device(dev):
                 for k in range(len(fs.inst)):
-                    self._layout(k, self._dev_in, self._din[k], to_dense=False)
+                    self._layout(k, self._dev_in, self._din[0][k], to_dense=False)
                 torch.cuda.current_stream(dev).synchronize()
-            for hb, db in zip(self._in_blocks, self._din):
+            for hb, db in zip(self._in_blocks, self._din[0]):
                 hb.copy_(db)
         n = len(fs.inst)
         words = fs._ctrl_size // 4
@@ -820,9 +825,14 @@ class HostStepper:
         self._h2d = torch.cuda.Stream(dev)
         self._d2h = torch.cuda.Stream(dev)
         self._stepped = torch.cuda.Event()
-        self._expanded = torch.cuda.Event()
         self._copied_in = torch.cuda.Event()
         self._copied_out = torch.cuda.Event()
+        # compact layout: per device set, the scatter that read it, its
+        # inbound copy, and the outbound copy that read its gathered result
+        self._expanded_set = [torch.cuda.Event(), torch.cuda.Event()]
+        self._in_set = [torch.cuda.Event(), torch.cuda.Event()]
+        self._out_set = [torch.cuda.Event(), torch.cuda.Event()]
+        self._n_steps = 0
         self._any = False
 
     def _layout(self, k: int, dense: list, block: torch.Tensor, to_dense: bool) -> None:
@@ -850,29 +860,33 @@ class HostStepper:
             self._step_dense()
             return
         comp = torch.cuda.current_stream(self.fs.device)
-        if self._any:
-            self._h2d.wait_event(self._expanded)
+        j = self._n_steps % 2
+        din, dout = self._din[j], self._dout[j]
+        if self._n_steps >= 2:
+            self._h2d.wait_event(self._expanded_set[j])
         with torch.cuda.stream(self._h2d):
-            for db, hb in zip(self._din, self._in_blocks):
+            for db, hb in zip(din, self._in_blocks):
                 db.copy_(hb, non_blocking=True)
-            self._copied_in.record(self._h2d)
-        comp.wait_event(self._copied_in)
+            self._in_set[j].record(self._h2d)
+        comp.wait_event(self._in_set[j])
         with torch.cuda.device(self.fs.device):
             for k in range(len(self.fs.inst)):
-                self._layout(k, self._dev_in, self._din[k], to_dense=True)
-            self._expanded.record(comp)
+                self._layout(k, self._dev_in, din[k], to_dense=True)
+            self._expanded_set[j].record(comp)
             self._cur.fill_(self.read)
             self.fs.step(1)
-            if self._any:
-                comp.wait_event(self._copied_out)
+            if self._n_steps >= 2:
+                comp.wait_event(self._out_set[j])
             for k in range(len(self.fs.inst)):
-                self._layout(k, self._dev_out, self._dout[k], to_dense=False)
+                self._layout(k, self._dev_out, dout[k], to_dense=False)
         self._stepped.record(comp)
         self._d2h.wait_event(self._stepped)
         with torch.cuda.stream(self._d2h):
-            for hb, db in zip(self._out_blocks, self._dout):
+            for hb, db in zip(self._out_blocks, dout):
                 hb.copy_(db, non_blocking=True)
+            self._out_set[j].record(self._d2h)
             self._copied_out.record(self._d2h)
+        self._n_steps += 1
         self._any = True
 
     def _step_dense(self) -> None:
