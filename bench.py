@@ -493,8 +493,8 @@ def first_order_rates(d: dict, dev, args, flush: torch.Tensor, stream, steps: in
     from hipims_b200.fused import FusedSolver
     from hipims_b200.scenarios import catchment_from
 
-    fs = FusedSolver(catchment_from(d), dtype=torch.float32, tile=(32, 32), device=dev,
-                     minb=5, order=1)
+    fs = FusedSolver(catchment_from(d), dtype=torch.float32, tile=(32, 64), device=dev,
+                     order=1)
     n = sum(i.n_valid for i in fs.inst)
     fs.step(SPINUP + args.warmup)
     torch.cuda.synchronize(dev)
@@ -510,7 +510,8 @@ def first_order_rates(d: dict, dev, args, flush: torch.Tensor, stream, steps: in
     ms = sum(a.elapsed_time(b) for a, b in ev) / steps
     value = n / (ms * 1e-3) / 1e9
     out = {"value": value, "unit": METRIC, "steps": steps, "ms_per_step": ms, "dtype": "f32",
-           "path": "FusedSolver(order=1): the two builds of the 1st-order step kernel, "
+           "path": "FusedSolver(order=1), 64 x 32 tiles, two cells per lane: the two builds "
+                   "of the 1st-order step kernel, "
                    "CUDA events per step, L2 flushed between steps"}
     del fs
     pl = plain_fp64_rate(d, dev, reference_kernels=True, order=1)
@@ -720,7 +721,7 @@ def adjoint_cost(dev, n: int = 1024, steps: int = 2000, K: int = 100, every: int
 
 
 def coupled_rate(dev, n: int = 8192, sim_seconds: float = 120.0, period: float = 60.0,
-                 agents: int = 100_000, tile=(32, 32), minb: int = 5) -> dict:
+                 agents: int = 100_000, tile=(32, 64), minb: int = 0) -> dict:
     """Config 5: an n x n catchment (1 m cells, rain 100 mm/h, Q_GIVEN inflow
     hydrograph on one edge) advanced by the fused FP32 step from a dry start,
     in the 1st-order scheme the reference's coupled server runs

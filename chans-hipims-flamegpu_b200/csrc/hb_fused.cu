@@ -1963,11 +1963,11 @@ int launch_rows_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
 // tiles on the caller's stream, both at once.
 // The general build keeps the register cap of 3 CTAs per SM (its ghost-face
 // branches spill under a tighter one); MINB caps the all-valid build.
-template <int TY, int MINB, bool SOURCES>
+template <int TY, int MINB, bool SOURCES, int ORDER = 2>
 int launch_pairs_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   using S = PairSmem<TY>;
-  auto *kg = pairs_step_kernel<TY, 3, SOURCES, 0>;
-  auto *ka = pairs_step_kernel<TY, MINB, SOURCES, 1>;
+  auto *kg = pairs_step_kernel<TY, 3, SOURCES, 0, ORDER>;
+  auto *ka = pairs_step_kernel<TY, MINB, SOURCES, 1, ORDER>;
   int rc = set_smem_attr(reinterpret_cast<const void *>(kg), (int)sizeof(S));
   if (!rc) rc = set_smem_attr(reinterpret_cast<const void *>(ka), (int)sizeof(S));
   if (rc) return rc;
@@ -2012,6 +2012,12 @@ int launch_pairs_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
 int launch_pairs(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   const int minb = (b->flags >> HB_FLAG_MINB_SHIFT) & 0xF;
   const bool src = (b->flags & HB_FLAG_SOURCES) != 0;
+  if (b->order == 1) {  // the 1st-order scheme: the all-valid build at 4 CTAs per SM
+    if (minb == 0 || minb == 4) return src ? launch_pairs_impl<32, 4, true, 1>(b, nsteps, st)
+                                           : launch_pairs_impl<32, 4, false, 1>(b, nsteps, st);
+    return set_error(HB_ERR_ARG, "hb_fused_step: the 1st-order 64-wide tiles are built for "
+                                 "4 CTAs per SM (minb 0 or 4), not %d", minb);
+  }
   if (minb == 3) return src ? launch_pairs_impl<32, 3, true>(b, nsteps, st)
                             : launch_pairs_impl<32, 3, false>(b, nsteps, st);
   if (minb == 0 || minb == 4) return src ? launch_pairs_impl<32, 4, true>(b, nsteps, st)
@@ -2137,9 +2143,9 @@ int prepare_impl(const hb_fused_batch *b, cudaStream_t st, CUtensorMap *host_map
     if (!pairs && (b->tile_x != kTW || (b->tile_y != 32 && b->tile_y != 64)))
       return set_error(HB_ERR_ARG, "hb_fused_prepare: rows kernel tiles are 32 wide, 32 or 64 "
                                    "high, or 64 wide and 32 high");
-    if (pairs && (b->dtype != HB_F32 || b->order != 2 || (b->flags & HB_FLAG_EXACT_FP32)))
+    if (pairs && (b->dtype != HB_F32 || (b->flags & HB_FLAG_EXACT_FP32)))
       return set_error(HB_ERR_ARG, "hb_fused_prepare: 64-wide tiles (two cells per lane) are "
-                                   "built for the FP32 2nd-order step");
+                                   "built for the FP32 step");
     int rc;
     if (host_maps) {
       rc = encode_maps(b, st, host_maps);
@@ -2260,7 +2266,9 @@ extern "C" int hb_fused_step(const hb_fused_batch *b, int nsteps, void *stream) 
   const int ty = b->tile_y, tx = b->tile_x;
   const bool exact = (b->flags & HB_FLAG_EXACT_FP32) != 0;
   if (uses_rows_kernel(b) && b->order == 1) {
-    // the 1st-order scheme (the coupled server's): FP32 32 x 32 tiles, FP64
+    // the 1st-order scheme (the coupled server's): FP32 64 x 32 tiles (two
+    // cells per lane) or 32 x 32 tiles, FP64 32 x 32 tiles
+    if (tx == kPW && ty == 32 && b->dtype == HB_F32 && !exact) return launch_pairs(b, nsteps, st);
     if (tx == kTW && ty == 32 && b->dtype == HB_F32 && !exact) {
       const int minb = (b->flags >> HB_FLAG_MINB_SHIFT) & 0xF;
       if (minb == 0) return launch_rows<float, 32, true, 1, 1>(b, nsteps, st);
@@ -2268,8 +2276,8 @@ extern "C" int hb_fused_step(const hb_fused_batch *b, int nsteps, void *stream) 
     }
     if (tx == kTW && ty == 32 && b->dtype == HB_F64)
       return launch_rows<double, 32, false, 1, 1>(b, nsteps, st);
-    return set_error(HB_ERR_ARG, "hb_fused_step: order 1 is built for 32 x 32 tiles, FP32 (fast, "
-                                 "minb 0 or 5) and FP64");
+    return set_error(HB_ERR_ARG, "hb_fused_step: order 1 is built for FP32 64 x 32 tiles (minb "
+                                 "0 or 4) and 32 x 32 tiles (minb 0 or 5), and FP64 32 x 32 tiles");
   }
   if (uses_rows_kernel(b) && tx == kPW) {
     if (ty == 32 && b->dtype == HB_F32 && !exact && b->order == 2) return launch_pairs(b, nsteps, st);

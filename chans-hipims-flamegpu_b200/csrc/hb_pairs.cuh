@@ -145,6 +145,11 @@ struct Fc2 {
 // momentum flux; ft is linear in the tangential discharge, so a caller that
 // passes +q instead of -q for it takes -ft.
 //
+// ORDER 2 raises the downhill edge level to the other's (the 2nd-order
+// hydrostatic step, :43-72); ORDER 1 averages the two edge levels when their
+// ordering is the reverse of the cells' (the 1st-order step,
+// HC/fluxCal_jh_modified_surface_Kernel.cu:96-139).
+//
 // The hydrostatic step runs with beds measured from the higher of the two edge
 // beds, o = max(Lz, Rz) (every operation of the scheme is invariant under a
 // common shift of z).  The upper edge then has bed 0 and its free surface is
@@ -152,6 +157,7 @@ struct Fc2 {
 // the last bit instead of being rounded at the scale of the bed step (6e-8 m
 // per 0.5 m of relief in FP32), which decided which side of h_small such a
 // cell fell on.
+template <int ORDER>
 __device__ __forceinline__ void face_core2(f2 ah, f2 bh, f2 bz, f2 Lh, f2 Lz0, f2 Lqn, f2 Lqt,
                                            f2 Rh, f2 Rz0, f2 Rqn, f2 Rqt, f2 &fh, f2 &fn,
                                            f2 &ft, f2 &sa, f2 &sb) {
@@ -164,16 +170,23 @@ __device__ __forceinline__ void face_core2(f2 ah, f2 bh, f2 bz, f2 Lh, f2 Lz0, f
   const f2 ir = pk(Rh.x < kHsF ? 0.f : rcpa(Rh.x), Rh.y < kHsF ? 0.f : rcpa(Rh.y));
   const f2 uL = mul2(Lqn, il), vL = mul2(Lqt, il);
   const f2 uR = mul2(Rqn, ir), vR = mul2(Rqt, ir);
-  // hydrostatic reconstruction, 2nd-order form
+  // hydrostatic reconstruction
   f2 Lw = add2(Lh, Lz), Rw = add2(Rh, Rz);
   {
     const float hix = fmaxf(wa.x, wb.x), lox = fminf(wa.x, wb.x);
     const float hiy = fmaxf(wa.y, wb.y), loy = fminf(wa.y, wb.y);
     Lw = pk(fmaxf(fminf(Lw.x, hix), lox), fmaxf(fminf(Lw.y, hiy), loy));
     Rw = pk(fmaxf(fminf(Rw.x, hix), lox), fmaxf(fminf(Rw.y, hiy), loy));
-    const float mx = fmaxf(Lw.x, Rw.x), my = fmaxf(Lw.y, Rw.y);
-    if (wa.x > wb.x) Lw.x = mx; else Rw.x = mx;
-    if (wa.y > wb.y) Lw.y = my; else Rw.y = my;
+    if constexpr (ORDER == 2) {
+      const float mx = fmaxf(Lw.x, Rw.x), my = fmaxf(Lw.y, Rw.y);
+      if (wa.x > wb.x) Lw.x = mx; else Rw.x = mx;
+      if (wa.y > wb.y) Lw.y = my; else Rw.y = my;
+    } else {
+      const f2 flip = mul2(sub2(wa, wb), sub2(Lw, Rw));
+      const f2 avg = mul2(add2(Lw, Rw), dup(0.5f));
+      if (flip.x < 0.f) Lw.x = Rw.x = avg.x;
+      if (flip.y < 0.f) Lw.y = Rw.y = avg.y;
+    }
   }
   const f2 Lz1 = sub2(Lw, Lh), Rz1 = sub2(Rw, Rh);
   const f2 zbm = pk(fmaxf(Lz1.x, Rz1.x), fmaxf(Lz1.y, Rz1.y));
@@ -232,10 +245,14 @@ __device__ __forceinline__ void face_core2(f2 ah, f2 bh, f2 bz, f2 Lh, f2 Lz0, f
 
 // Two interior faces between valid cells A (minus side: west, or south) and
 // B (plus side) along DIR (0: normal +x; 1: normal +y, towards the row
-// above), from the cells and their MUSCL slopes along DIR
-// (HC/flucCal_2ndOrder_jh_improved_Kernel.cu:83-107, 410-485).  The frame
-// measures beds from A's bed.  A face whose two cells are both dry is zero.
-template <int DIR>
+// above), from the cells and their minmod slopes along DIR.  ORDER 2: MUSCL
+// edge states (HC/flucCal_2ndOrder_jh_improved_Kernel.cu:83-107, 410-485);
+// ORDER 1: the cells themselves, only the bed taking half its slope on a side
+// whose neighbour across the face is wet
+// (HC/fluxCal_jh_modified_surface_Kernel.cu:577-593; only sA.z, sB.z are
+// read).  The frame measures beds from A's bed.  A face whose two cells are
+// both dry is zero.
+template <int DIR, int ORDER = 2>
 __device__ __forceinline__ Fc2 face2(const Cel2 &A, const Cel2 &B, const Slp2 &sA,
                                      const Slp2 &sB) {
   Fc2 o;
@@ -245,24 +262,43 @@ __device__ __forceinline__ Fc2 face2(const Cel2 &A, const Cel2 &B, const Slp2 &s
     return o;
   }
   const f2 bz = sub2(B.z, A.z);
-  const f2 Lh = fma2(dup(0.5f), sA.h, A.h), Lz = mul2(dup(0.5f), sA.z);
-  f2 Lqx = fma2(dup(0.5f), sA.qx, A.qx), Lqy = fma2(dup(0.5f), sA.qy, A.qy);
-  const f2 Rh = fma2(dup(-0.5f), sB.h, B.h), Rz = fma2(dup(-0.5f), sB.z, bz);
-  f2 Rqx = fma2(dup(-0.5f), sB.qx, B.qx), Rqy = fma2(dup(-0.5f), sB.qy, B.qy);
-  // a dry cell's edges carry no discharge
-  if (A.h.x < kHsF) Lqx.x = Lqy.x = 0.f;
-  if (A.h.y < kHsF) Lqx.y = Lqy.y = 0.f;
-  if (B.h.x < kHsF) Rqx.x = Rqy.x = 0.f;
-  if (B.h.y < kHsF) Rqx.y = Rqy.y = 0.f;
+  f2 Lh, Lz, Lqx, Lqy, Rh, Rz, Rqx, Rqy;
+  if constexpr (ORDER == 2) {
+    Lh = fma2(dup(0.5f), sA.h, A.h);
+    Lz = mul2(dup(0.5f), sA.z);
+    Lqx = fma2(dup(0.5f), sA.qx, A.qx);
+    Lqy = fma2(dup(0.5f), sA.qy, A.qy);
+    Rh = fma2(dup(-0.5f), sB.h, B.h);
+    Rz = fma2(dup(-0.5f), sB.z, bz);
+    Rqx = fma2(dup(-0.5f), sB.qx, B.qx);
+    Rqy = fma2(dup(-0.5f), sB.qy, B.qy);
+    // a dry cell's edges carry no discharge
+    if (A.h.x < kHsF) Lqx.x = Lqy.x = 0.f;
+    if (A.h.y < kHsF) Lqx.y = Lqy.y = 0.f;
+    if (B.h.x < kHsF) Rqx.x = Rqy.x = 0.f;
+    if (B.h.y < kHsF) Rqx.y = Rqy.y = 0.f;
+  } else {
+    Lh = A.h;
+    Rh = B.h;
+    Lqx = A.qx;
+    Lqy = A.qy;
+    Rqx = B.qx;
+    Rqy = B.qy;
+    const f2 lz = mul2(dup(0.5f), sA.z), rz = fma2(dup(-0.5f), sB.z, bz);
+    Lz = pk(B.h.x > kHsF ? lz.x : 0.f, B.h.y > kHsF ? lz.y : 0.f);
+    Rz = pk(A.h.x > kHsF ? rz.x : bz.x, A.h.y > kHsF ? rz.y : bz.y);
+  }
   f2 fn, ft;
   if constexpr (DIR == 0) {
-    face_core2(A.h, B.h, bz, Lh, Lz, Lqx, Lqy, Rh, Rz, Rqx, Rqy, o.fh, fn, ft, o.sa, o.sb);
+    face_core2<ORDER>(A.h, B.h, bz, Lh, Lz, Lqx, Lqy, Rh, Rz, Rqx, Rqy, o.fh, fn, ft, o.sa,
+                      o.sb);
     o.fx = fn;
     o.fy = ft;
   } else {
     // normal +y, tangent -x: the tangential discharge is passed as +qx, so
     // the face's x-momentum flux (-ft of the -qx form) is ft
-    face_core2(A.h, B.h, bz, Lh, Lz, Lqy, Lqx, Rh, Rz, Rqy, Rqx, o.fh, fn, ft, o.sa, o.sb);
+    face_core2<ORDER>(A.h, B.h, bz, Lh, Lz, Lqy, Lqx, Rh, Rz, Rqy, Rqx, o.fh, fn, ft, o.sa,
+                      o.sb);
     o.fx = ft;
     o.fy = fn;
   }
@@ -280,6 +316,7 @@ __device__ __forceinline__ Fc2 face2(const Cel2 &A, const Cel2 &B, const Slp2 &s
 struct Ghost1 {
   float fh, fx, fy, sc;
 };
+template <int ORDER>
 __device__ __noinline__ Ghost1 ghost_face1(float ch, float cqx, float cqy, float cz, int type,
                                            const double *bcv, float datum, int side) {
   Ghost1 r{0.f, 0.f, 0.f, 0.f};
@@ -294,7 +331,8 @@ __device__ __noinline__ Ghost1 ghost_face1(float ch, float cqx, float cqy, float
   const float hb = (float)bcv[0];
   const float wlb = (float)(bcv[1] - (double)datum) - cz;
   const float qxb = (float)bcv[2], qyb = (float)bcv[3];
-  if (!ghost(type, false, Cl, n0, n1, hb, wlb, qxb, qyb, G)) return r;
+  // FALL (type 9) is a ghost of the 1st-order scheme only
+  if (!ghost(type, ORDER == 1, Cl, n0, n1, hb, wlb, qxb, qyb, G)) return r;
   if (Cl.h < kHsF && G.h < kHsF) return r;
   // discharges in C's outward frame (normal, tangential)
   float cqn, cqt, gqn, gqt;
@@ -310,8 +348,8 @@ __device__ __noinline__ Ghost1 ghost_face1(float ch, float cqx, float cqy, float
   f2 fh, fn, ft, sa, sb;
   // (every ghost has G.wl = G.z + G.h in C's frame, the free surface the
   // face core forms from the bed and the depth)
-  face_core2(dup(Cl.h), dup(G.h), dup(G.z), dup(Cl.h), dup(0.f), dup(cqn), dup(cqt), dup(G.h),
-             dup(G.z), dup(gqn), dup(gqt), fh, fn, ft, sa, sb);
+  face_core2<ORDER>(dup(Cl.h), dup(G.h), dup(G.z), dup(Cl.h), dup(0.f), dup(cqn), dup(cqt),
+                    dup(G.h), dup(G.z), dup(gqn), dup(gqt), fh, fn, ft, sa, sb);
   r.sc = sa.x;
   if (side == 0) {  // C is the west side
     r.fh = fh.x; r.fx = fn.x; r.fy = ft.x;
@@ -434,11 +472,11 @@ __device__ __forceinline__ Slp2 yslope2(const Cel2 &c, const Cel2 &s, f2 vs, con
 // build fixed up per face: va / vb say whether side A / B of each face is a
 // valid cell; ca / cb are their codes.  DIR 0: A is the west side, DIR 1 the
 // south side.
-template <int DIR, bool ALLV, int TY>
+template <int DIR, bool ALLV, int TY, int ORDER = 2>
 __device__ __forceinline__ Fc2 face_pair(const PairSmem<TY> &s, const Cel2 &A, const Cel2 &B,
                                          const Slp2 &sA, const Slp2 &sB, uint8_t ca0,
                                          uint8_t ca1, uint8_t cb0, uint8_t cb1, float datum) {
-  Fc2 o = face2<DIR>(A, B, sA, sB);
+  Fc2 o = face2<DIR, ORDER>(A, B, sA, sB);
   if constexpr (!ALLV) {
     const bool va0 = is_valid(ca0), va1 = is_valid(ca1), vb0 = is_valid(cb0), vb1 = is_valid(cb1);
     if (!(va0 && vb0) || !(va1 && vb1)) {
@@ -450,13 +488,15 @@ __device__ __forceinline__ Fc2 face_pair(const PairSmem<TY> &s, const Cel2 &A, c
         float sa = 0.f, sb = 0.f;
         if (va) {
           const int cls = (c ? ca1 : ca0) >> 4;
-          gr = ghost_face1(c ? A.h.y : A.h.x, c ? A.qx.y : A.qx.x, c ? A.qy.y : A.qy.x,
-                           c ? A.z.y : A.z.x, s.bctype[cls], s.bc[cls], datum, DIR == 0 ? 0 : 1);
+          gr = ghost_face1<ORDER>(c ? A.h.y : A.h.x, c ? A.qx.y : A.qx.x, c ? A.qy.y : A.qy.x,
+                                  c ? A.z.y : A.z.x, s.bctype[cls], s.bc[cls], datum,
+                                  DIR == 0 ? 0 : 1);
           sa = gr.sc;
         } else if (vb) {
           const int cls = (c ? cb1 : cb0) >> 4;
-          gr = ghost_face1(c ? B.h.y : B.h.x, c ? B.qx.y : B.qx.x, c ? B.qy.y : B.qy.x,
-                           c ? B.z.y : B.z.x, s.bctype[cls], s.bc[cls], datum, DIR == 0 ? 2 : 3);
+          gr = ghost_face1<ORDER>(c ? B.h.y : B.h.x, c ? B.qx.y : B.qx.x, c ? B.qy.y : B.qy.x,
+                                  c ? B.z.y : B.z.x, s.bctype[cls], s.bc[cls], datum,
+                                  DIR == 0 ? 2 : 3);
           sb = gr.sc;
         }
         if (c) {
@@ -471,7 +511,7 @@ __device__ __forceinline__ Fc2 face_pair(const PairSmem<TY> &s, const Cel2 &A, c
 }
 
 // ===========================================================================
-// One tile of a step (FP32, 2nd order): stage it, evaluate its faces, update
+// One tile of a step (FP32, scheme ORDER 2 or 1): stage it, evaluate its faces, update
 // its cells, write its partial sums, and close its group / finalize its
 // instance when it is the last.  PATH 0: a general tile (no-data cells, ghost
 // faces or the cell-0 rule's cell in reach); PATH 1: an all-valid tile.
@@ -481,7 +521,7 @@ __device__ __forceinline__ Fc2 face_pair(const PairSmem<TY> &s, const Cel2 &A, c
 // One tile: en = its TileEntry (en.tile < 0: ~tile of a general tile that
 // holds no valid cell, which loads nothing and adds a zero partial to its
 // group).
-template <int TY, bool SOURCES, int PATH>
+template <int TY, bool SOURCES, int PATH, int ORDER = 2>
 __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, const TileEntry en,
                                           const hb_instance *__restrict__ insts,
                                           TilePartial *__restrict__ partials,
@@ -599,7 +639,7 @@ __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, cons
       xslope1<TY, ALLV>(V, i + 1, 64, b1[0], b1[1], b1[2], b1[3]);
       const Slp2 sA{pk(a[0], a1[0]), pk(a[1], a1[1]), pk(a[2], a1[2]), pk(a[3], a1[3])};
       const Slp2 sB{pk(b[0], b1[0]), pk(b[1], b1[1]), pk(b[2], b1[2]), pk(b[3], b1[3])};
-      const Fc2 f = face_pair<0, ALLV>(s, V.vpair(i, 63), V.vpair(i, 64), sA, sB,
+      const Fc2 f = face_pair<0, ALLV, TY, ORDER>(s, V.vpair(i, 63), V.vpair(i, 64), sA, sB,
                                        V.code(i, 63), V.code(i + 1, 63), V.code(i, 64),
                                        V.code(i + 1, 64), datum_tile);
       s.xe[i][0] = f.fh.x; s.xe[i][1] = f.fx.x; s.xe[i][2] = f.fy.x; s.xe[i][3] = f.sa.x;
@@ -610,10 +650,12 @@ __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, cons
     for (int i = lane; i < TY; i += 32) {
       float sh, sz, sqx, sqy;
       xslope1<TY, ALLV>(V, i, -1, sh, sz, sqx, sqy);
-      s.sxw[i][0] = sh;
       s.sxw[i][1] = sz;
-      s.sxw[i][2] = sqx;
-      s.sxw[i][3] = sqy;
+      if constexpr (ORDER == 2) {  // the 1st-order faces read only the bed's slope
+        s.sxw[i][0] = sh;
+        s.sxw[i][2] = sqx;
+        s.sxw[i][3] = sqy;
+      }
     }
   }
 
@@ -656,7 +698,7 @@ __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, cons
       const Slp2 syN = yslope2<ALLV>(N, C, vC, NN, vpair(r0 - 2));
       syC = yslope2<ALLV>(C, S1, vpair(r0 + 1), N, vN);
       // face between rows r0-1 (north, B) and r0 (south, A)
-      nf = face_pair<1, ALLV>(s, C, N, syC, syN, V.code(r0, j0), V.code(r0, j0 + 1),
+      nf = face_pair<1, ALLV, TY, ORDER>(s, C, N, syC, syN, V.code(r0, j0), V.code(r0, j0 + 1),
                               V.code(r0 - 1, j0), V.code(r0 - 1, j0 + 1), datum_tile);
       Nh = N.h;
     }
@@ -703,15 +745,19 @@ __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, cons
         sxa[q] = slope1(cA[q], vWb ? Wv[q] : cA[q], vBb ? cB[q] : cA[q]);
         sxb[q] = slope1(cB[q], vAb ? cA[q] : cB[q], vEb ? Ev[q] : cB[q]);
       }
-      // slope of col 2j-1 from the west lane (lane 0: the pre-pass)
-      float sw[4];
+      // slope of col 2j-1 from the west lane (lane 0: the pre-pass); the
+      // 1st-order faces read only the bed's
+      float sw[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-      for (int q = 0; q < 4; q++) sw[q] = __shfl_up_sync(0xffffffffu, sxb[q], 1);
+      for (int q = 0; q < 4; q++)
+        if (ORDER == 2 || q == 3) sw[q] = __shfl_up_sync(0xffffffffu, sxb[q], 1);
       if (lane == 0) {
-        sw[0] = s.sxw[i][0];
         sw[3] = s.sxw[i][1];
-        sw[1] = s.sxw[i][2];
-        sw[2] = s.sxw[i][3];
+        if constexpr (ORDER == 2) {
+          sw[0] = s.sxw[i][0];
+          sw[1] = s.sxw[i][2];
+          sw[2] = s.sxw[i][3];
+        }
       }
       // --- west faces of a and b: (2j-1 | 2j) and (2j | 2j+1)
       f2 Px_h, Px_x, Px_y;  // x-direction flux differences (west - east) of the pair
@@ -721,7 +767,8 @@ __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, cons
         const Cel2 Aw{pk(Wv[0], C.h.x), pk(Wv[1], C.qx.x), pk(Wv[2], C.qy.x), pk(Wv[3], C.z.x)};
         const Slp2 sAw{pk(sw[0], sxa[0]), pk(sw[3], sxa[3]), pk(sw[1], sxa[1]), pk(sw[2], sxa[2])};
         const Slp2 sBw{pk(sxa[0], sxb[0]), pk(sxa[3], sxb[3]), pk(sxa[1], sxb[1]), pk(sxa[2], sxb[2])};
-        const Fc2 wf = face_pair<0, ALLV>(s, Aw, C, sAw, sBw, kW, kA, kA, kB, datum_tile);
+        const Fc2 wf = face_pair<0, ALLV, TY, ORDER>(s, Aw, C, sAw, sBw, kW, kA, kA, kB,
+                                                     datum_tile);
         // east faces: a's is the lane's second west face; b's comes from lane j+1
         float e_h = __shfl_down_sync(0xffffffffu, wf.fh.x, 1);
         float e_x = __shfl_down_sync(0xffffffffu, wf.fx.x, 1);
@@ -754,7 +801,7 @@ __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, cons
           kSa = V.code(i + 1, j0);
           kSb = V.code(i + 1, j0 + 1);
         }
-        sf = face_pair<1, ALLV>(s, Sx, C, syS, syC, kSa, kSb, kA, kB, datum_tile);
+        sf = face_pair<1, ALLV, TY, ORDER>(s, Sx, C, syS, syC, kSa, kSb, kA, kB, datum_tile);
       }
 
       // --- cell updates
@@ -986,7 +1033,7 @@ __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, cons
 
 // The step kernel: one launch per step and build, one CTA per tile by
 // default (a positive grid loops over the build's tiles).
-template <int TY, int MINB, bool SOURCES, int PATH>
+template <int TY, int MINB, bool SOURCES, int PATH, int ORDER = 2>
 __global__ void __launch_bounds__(kRowsNT, MINB)
 pairs_step_kernel(const hb_instance *__restrict__ insts, const TileEntry *__restrict__ list,
                   const int n_list, TilePartial *__restrict__ partials,
@@ -1003,8 +1050,8 @@ pairs_step_kernel(const hb_instance *__restrict__ insts, const TileEntry *__rest
   __syncthreads();
   unsigned phase = 0;
   for (int k = blockIdx.x; k < n_list; k += gridDim.x)
-    if (!pair_tile<TY, SOURCES, PATH>(s, phase, list[k], insts, partials, gparts, gcount, bct,
-                                      maps))
+    if (!pair_tile<TY, SOURCES, PATH, ORDER>(s, phase, list[k], insts, partials, gparts, gcount,
+                                             bct, maps))
       return;
 }
 

@@ -323,11 +323,11 @@ class FusedSolver:
 
     order 2 (default): the reference's 2nd-order scheme (MUSCL, `secondOrder`
     True); order 1: its 1st-order scheme (`secondOrder` False, the coupled
-    server's choice, CHANS-HiPIMS_server.py), rows kernel with 32 x 32 tiles.
+    server's choice, CHANS-HiPIMS_server.py).
 
-    tile = (rows, cols): (32, 64) runs two cells per lane (FP32 2nd order, the
-    default there); (32, 32) and (64, 32) one cell per lane (every dtype and
-    order).
+    tile = (rows, cols): (32, 64) runs two cells per lane (FP32, either order:
+    the default there); (32, 32) and (64, 32) one cell per lane (every dtype
+    and order).
 
     origin: rows and columns of no-data the kernels see above and left of each
     catchment, i.e. where the tile grid starts (results are given back in the
@@ -352,9 +352,9 @@ class FusedSolver:
         self.dtype = dtype
         self.order = order
         if tile is None:
-            # FP32 2nd order (not exact_fp32): 32 x 64 tiles, two cells per lane;
+            # FP32 (not exact_fp32): 32 x 64 tiles, two cells per lane;
             # otherwise the 32 x 32 row-walking tiles
-            pairs = dtype == torch.float32 and kernel == "rows" and order == 2 and not exact_fp32
+            pairs = dtype == torch.float32 and kernel == "rows" and not exact_fp32
             tile = (32, 64) if pairs else (32, 32)
         self.tile = tuple(tile)
         if origin is None:

@@ -84,9 +84,11 @@ def test_first_order_fp64_mixed_boundaries_with_fall(cuda, seed):
         assert (max(err.values()) if k <= 6 else err["h"]) < tol, (k, err)
 
 
-def test_first_order_fp32_dam_break(cuda):
+@pytest.mark.parametrize("tile,minb", [((32, 32), 5), ((32, 64), 0)])
+def test_first_order_fp32_dam_break(cuda, tile, minb):
     """256 x 256 dam break in FP32 against the FP64 oracle at the same
-    simulated times; uniform along y, so qy stays exactly 0."""
+    simulated times; uniform along y, so qy stays exactly 0.  Both step
+    kernels: one cell per lane (32 x 32) and two (32 x 64)."""
     from hipims_b200 import scenarios as S
     from hipims_b200.fused import FusedSolver
 
@@ -96,16 +98,17 @@ def test_first_order_fp32_dam_break(cuda):
     ref = O.Sim(d, order=1)
     ref.run(200)
     fs = FusedSolver(catchment(d, dt_replay=dts), dtype=torch.float32, device=cuda, order=1,
-                     minb=5)
+                     tile=tile, minb=minb)
     fs.step(200)
     got = fs.compacted()
     err = float(np.abs(got["h"] - ref.h).max())
-    print("1st-order FP32 dam break, 200 steps, max|dh|", err)
+    print("1st-order FP32 dam break", tile, "200 steps, max|dh|", err)
     assert np.abs(got["qy"]).max() == 0.0
     assert err <= 1e-4
 
 
-def test_first_order_fp32_urban_rain(cuda):
+@pytest.mark.parametrize("tile", [(32, 32), (32, 64)])
+def test_first_order_fp32_urban_rain(cuda, tile):
     """Rain on the urban DEM (buildings, two Manning zones, open ring, dry
     start) in FP32 against the FP64 oracle at the same simulated times."""
     from hipims_b200 import scenarios as S
@@ -116,10 +119,11 @@ def test_first_order_fp32_urban_rain(cuda):
     dts = sim.run_record(25)
     ref = O.Sim(d, order=1)
     ref.run(25)
-    fs = FusedSolver(catchment(d, dt_replay=dts), dtype=torch.float32, device=cuda, order=1)
+    fs = FusedSolver(catchment(d, dt_replay=dts), dtype=torch.float32, device=cuda, order=1,
+                     tile=tile)
     fs.step(25)
     err = float(np.abs(fs.compacted()["h"] - ref.h).max())
-    print("1st-order urban FP32 vs FP64 oracle after 25 steps, max|dh|", err)
+    print("1st-order urban FP32", tile, "vs FP64 oracle after 25 steps, max|dh|", err)
     assert err <= 2e-4
 
 
@@ -130,10 +134,30 @@ def test_first_order_strips_reproduce_the_undivided_run(cuda):
 
     d = S.urban_catchment(192, dx=2.0, seed=8, rain_mm_h=120.0)
     c = S.catchment_from(d)
-    one = FusedSolver(c, dtype=torch.float32, device=cuda, order=1)
+    one = FusedSolver(c, dtype=torch.float32, device=cuda, order=1, origin=(0, 0))
     st = StripSolver(c, 3, dtype=torch.float32, device=cuda, order=1)
     one.step(40)
     st.step(40)
     a, b = one.state(), st.state()
     for f in ("h", "qx", "qy", "h_max"):
         assert torch.equal(a[f], b[f]), f
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+@pytest.mark.parametrize("tile", [(32, 32), (32, 64)])
+def test_first_order_fp32_mixed_boundaries_with_fall(cuda, seed, tile):
+    """FP32 1st order on every ghost type FALL included, station rain off,
+    against the FP64 oracle with its dt sequence replayed (both kernels)."""
+    from hipims_b200.fused import FusedSolver
+
+    d = G.mixed_bc_case(200 + seed, 1)
+    d.pop("rain_mask")
+    d["rain"] = np.array([[0.0, 2e-4], [1.0, 5e-4], [10.0, 0.0]])
+    sim = O.Sim(d, order=1)
+    dts = sim.run_record(8)
+    fs = FusedSolver(catchment(d, dt_replay=dts), dtype=torch.float32, device=cuda, order=1,
+                     tile=tile)
+    fs.step(8)
+    err = compare(fs, sim)
+    print("1st-order mixed bc FP32", tile, "vs oracle after 8 steps:", err)
+    assert err["h"] < 1e-4 and err["qx"] < 1e-4 and err["qy"] < 1e-4, err
