@@ -157,17 +157,26 @@ struct Fc2 {
 // the last bit instead of being rounded at the scale of the bed step (6e-8 m
 // per 0.5 m of relief in FP32), which decided which side of h_small such a
 // cell fell on.
+//
+// The edge discharges enter only through the edge velocities, so a dry cell's
+// zero edge discharge is applied there: the velocity factor of an edge is 0
+// when its depth or its cell's depth is below h_small.  dd0 / dd1: the two
+// cells of that face are both dry; its fluxes are zero (with those of a face
+// whose reconstructed depths are both below h_small).
 template <int ORDER>
 __device__ __forceinline__ void face_core2(f2 ah, f2 bh, f2 bz, f2 Lh, f2 Lz0, f2 Lqn, f2 Lqt,
                                            f2 Rh, f2 Rz0, f2 Rqn, f2 Rqt, f2 &fh, f2 &fn,
-                                           f2 &ft, f2 &sa, f2 &sb) {
+                                           f2 &ft, f2 &sa, f2 &sb, bool dd0 = false,
+                                           bool dd1 = false) {
   const f2 o = pk(fmaxf(Lz0.x, Rz0.x), fmaxf(Lz0.y, Rz0.y));
   const f2 Lz = sub2(Lz0, o), Rz = sub2(Rz0, o);   // one of the two is exactly 0
   const f2 bzo = sub2(bz, o);                       // the plus cell's bed
   const f2 wa = sub2(ah, o), wb = add2(bzo, bh);    // the cells' free surfaces
   // velocities of the edge states
-  const f2 il = pk(Lh.x < kHsF ? 0.f : rcpa(Lh.x), Lh.y < kHsF ? 0.f : rcpa(Lh.y));
-  const f2 ir = pk(Rh.x < kHsF ? 0.f : rcpa(Rh.x), Rh.y < kHsF ? 0.f : rcpa(Rh.y));
+  const f2 il = pk(Lh.x < kHsF || ah.x < kHsF ? 0.f : rcpa(Lh.x),
+                   Lh.y < kHsF || ah.y < kHsF ? 0.f : rcpa(Lh.y));
+  const f2 ir = pk(Rh.x < kHsF || bh.x < kHsF ? 0.f : rcpa(Rh.x),
+                   Rh.y < kHsF || bh.y < kHsF ? 0.f : rcpa(Rh.y));
   const f2 uL = mul2(Lqn, il), vL = mul2(Lqt, il);
   const f2 uR = mul2(Rqn, ir), vR = mul2(Rqt, ir);
   // hydrostatic reconstruction
@@ -225,11 +234,13 @@ __device__ __forceinline__ void face_core2(f2 ah, f2 bh, f2 bz, f2 Lh, f2 Lz0, f
 #pragma unroll
   for (int c = 0; c < 2; c++) {
     const float sl = c ? sL.y : sL.x, sr = c ? sR.y : sR.x, sm = c ? sM.y : sM.x;
+    // the reference's chain sL >= 0 / sL < 0 <= sM / sM < 0 <= sR / else,
+    // with sL finite (it is, for a finite state)
     const bool left = 0.f <= sl;
-    const bool midL = !left && (sl < 0.f && 0.f <= sm);
-    const bool midR = !left && !midL && (sm < 0.f && 0.f <= sr);
+    const bool midL = !left && 0.f <= sm;
+    const bool midR = !left && sm < 0.f && 0.f <= sr;
     const bool mid = midL || midR;
-    const bool dry = (c ? hL.y : hL.x) < kHsF && (c ? hR.y : hR.x) < kHsF;
+    const bool dry = ((c ? hL.y : hL.x) < kHsF && (c ? hR.y : hR.x) < kHsF) || (c ? dd1 : dd0);
     float h_ = left ? (c ? hfL.y : hfL.x) : (mid ? (c ? hfM.y : hfM.x) : (c ? hfR.y : hfR.x));
     float n_ = left ? (c ? nfL.y : nfL.x) : (mid ? (c ? nfM.y : nfM.x) : (c ? nfR.y : nfR.x));
     float t_ = left ? (c ? tfL.y : tfL.x)
@@ -272,11 +283,8 @@ __device__ __forceinline__ Fc2 face2(const Cel2 &A, const Cel2 &B, const Slp2 &s
     Rz = fma2(dup(-0.5f), sB.z, bz);
     Rqx = fma2(dup(-0.5f), sB.qx, B.qx);
     Rqy = fma2(dup(-0.5f), sB.qy, B.qy);
-    // a dry cell's edges carry no discharge
-    if (A.h.x < kHsF) Lqx.x = Lqy.x = 0.f;
-    if (A.h.y < kHsF) Lqx.y = Lqy.y = 0.f;
-    if (B.h.x < kHsF) Rqx.x = Rqy.x = 0.f;
-    if (B.h.y < kHsF) Rqx.y = Rqy.y = 0.f;
+    // a dry cell's edges carry no discharge: face_core2 takes their
+    // velocities as 0
   } else {
     Lh = A.h;
     Rh = B.h;
@@ -291,19 +299,19 @@ __device__ __forceinline__ Fc2 face2(const Cel2 &A, const Cel2 &B, const Slp2 &s
   f2 fn, ft;
   if constexpr (DIR == 0) {
     face_core2<ORDER>(A.h, B.h, bz, Lh, Lz, Lqx, Lqy, Rh, Rz, Rqx, Rqy, o.fh, fn, ft, o.sa,
-                      o.sb);
+                      o.sb, dd0, dd1);
     o.fx = fn;
     o.fy = ft;
   } else {
     // normal +y, tangent -x: the tangential discharge is passed as +qx, so
     // the face's x-momentum flux (-ft of the -qx form) is ft
     face_core2<ORDER>(A.h, B.h, bz, Lh, Lz, Lqy, Lqx, Rh, Rz, Rqy, Rqx, o.fh, fn, ft, o.sa,
-                      o.sb);
+                      o.sb, dd0, dd1);
     o.fx = ft;
     o.fy = fn;
   }
-  if (dd0) o.fh.x = o.fx.x = o.fy.x = o.sa.x = o.sb.x = 0.f;
-  if (dd1) o.fh.y = o.fx.y = o.fy.y = o.sa.y = o.sb.y = 0.f;
+  if (dd0) o.sa.x = o.sb.x = 0.f;  // the fluxes: face_core2
+  if (dd1) o.sa.y = o.sb.y = 0.f;
   return o;
 }
 
@@ -904,7 +912,7 @@ __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, cons
           if (hh < kHsF) {
             qx = 0.f;
             qy = 0.f;
-            if (c) { sgh.y = 0.f; ih.y = 0.f; } else { sgh.x = 0.f; ih.x = 0.f; }
+            // (sgh, ih of a dry cell: the CFL speed below skips dry cells)
             continue;
           }
           if (!((c ? nman.y : nman.x) > 0.f)) continue;
