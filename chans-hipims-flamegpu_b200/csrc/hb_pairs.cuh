@@ -68,15 +68,10 @@ __device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
       : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
   return r;
 }
-// scalar forms, used where a value is formed for one cell only (x-slopes)
+// scalar form, used where a value is formed for one cell only (x-slopes)
 __device__ __forceinline__ float sub1(float a, float b) {
   float r;
   asm("sub.rn.ftz.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
-  return r;
-}
-__device__ __forceinline__ float mul1(float a, float b) {
-  float r;
-  asm("mul.rn.ftz.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
   return r;
 }
 // approximate reciprocal, square root, base-2 logarithm and exponential (the
@@ -107,20 +102,23 @@ constexpr float kHsF = 1.0e-6f;          // h_small
 constexpr float kGF = 9.81f;             // g
 constexpr float kHalfGF = 0.5f * 9.81f;  // exact: a power-of-two scaling of g
 
-// minmod(d1, d2) given p = d1 * d2 (HC/flucCal_2ndOrder_jh_improved_Kernel.cu:74-81)
-__device__ __forceinline__ float mmod(float d1, float d2, float p) {
-  return p <= 0.f ? 0.f : (fabsf(d1) < fabsf(d2) ? d1 : d2);
+// minmod(d1, d2) (HC/flucCal_2ndOrder_jh_improved_Kernel.cu:74-81): 0 when
+// the signs differ, else the one of smaller magnitude.  The reference tests
+// the sign of d1 * d2 in FP64; formed by min and max here (four ALU
+// operations, no product), so differences below 1e-19, whose FP32 product
+// would flush to zero, keep their sign test too.
+__device__ __forceinline__ float mmod(float d1, float d2) {
+  return fmaxf(fminf(d1, d2), fminf(0.f, fmaxf(d1, d2)));
 }
 // slope of c between its minus-side neighbour m and plus-side neighbour p
 // (x-slopes: one cell at a time)
 __device__ __forceinline__ float slope1(float c, float m, float p) {
-  const float d1 = sub1(c, m), d2 = sub1(p, c);
-  return mmod(d1, d2, mul1(d1, d2));
+  return mmod(sub1(c, m), sub1(p, c));
 }
 // the same for a vertical pair of cells (y-slopes)
 __device__ __forceinline__ f2 slope2(f2 c, f2 m, f2 p) {
-  const f2 d1 = sub2(c, m), d2 = sub2(p, c), q = mul2(d1, d2);
-  return pk(mmod(d1.x, d2.x, q.x), mmod(d1.y, d2.y, q.y));
+  const f2 d1 = sub2(c, m), d2 = sub2(p, c);
+  return pk(mmod(d1.x, d2.x), mmod(d1.y, d2.y));
 }
 
 struct Cel2 {
