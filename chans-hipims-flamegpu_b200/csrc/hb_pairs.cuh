@@ -205,8 +205,7 @@ __device__ __forceinline__ void face_core2(f2 ah, f2 bh, f2 bz, f2 Lh, f2 Lz0, f
   sa = mul2(mul2(dup(kHalfGF), add2(ah, hL)), add2(zL, o));  // zL - (the minus cell's bed, -o)
   sb = mul2(mul2(dup(kHalfGF), add2(bh, hR)), sub2(zR, bzo));
   // HLLC
-  const f2 qnL = mul2(uL, hL), qtL = mul2(vL, hL);
-  const f2 qnR = mul2(uR, hR), qtR = mul2(vR, hR);
+  const f2 qnL = mul2(uL, hL), qnR = mul2(uR, hR);
   const f2 gL = mul2(dup(kGF), hL), gR = mul2(dup(kGF), hR);
   const f2 aL = pk(sqrta(gL.x), sqrta(gL.y)), aR = pk(sqrta(gR.x), sqrta(gR.y));
   const f2 base = fma2(add2(aL, aR), dup(0.5f), mul2(sub2(uL, uR), dup(0.25f)));
@@ -219,7 +218,6 @@ __device__ __forceinline__ void face_core2(f2 ah, f2 bh, f2 bz, f2 Lh, f2 Lz0, f
   const f2 hfL = qnL, hfR = qnR;
   const f2 nfL = fma2(uL, qnL, mul2(mul2(dup(kHalfGF), hL), hL));
   const f2 nfR = fma2(uR, qnR, mul2(mul2(dup(kHalfGF), hR), hR));
-  const f2 tfL = mul2(uL, qtL), tfR = mul2(uR, qtR);
   const f2 pR = mul2(hR, sub2(uR, sR)), pL = mul2(hL, sub2(uL, sL));
   const f2 num = sub2(mul2(sL, pR), mul2(sR, pL)), den = sub2(pR, pL);
   const f2 sM = mul2(num, pk(rcpa(den.x), rcpa(den.y)));
@@ -227,8 +225,8 @@ __device__ __forceinline__ void face_core2(f2 ah, f2 bh, f2 bz, f2 Lh, f2 Lz0, f
   const f2 inv = pk(rcpa(dS.x), rcpa(dS.y));
   const f2 sLR = mul2(sL, sR);
   const f2 hfM = mul2(fma2(sLR, sub2(hR, hL), sub2(mul2(sR, hfL), mul2(sL, hfR))), inv);
+  f2 vU;
   const f2 nfM = mul2(fma2(sLR, sub2(qnR, qnL), sub2(mul2(sR, nfL), mul2(sL, nfR))), inv);
-  const f2 tML = mul2(hfM, vL), tMR = mul2(hfM, vR);
 #pragma unroll
   for (int c = 0; c < 2; c++) {
     const float sl = c ? sL.y : sL.x, sr = c ? sR.y : sR.x, sm = c ? sM.y : sM.x;
@@ -241,15 +239,18 @@ __device__ __forceinline__ void face_core2(f2 ah, f2 bh, f2 bz, f2 Lh, f2 Lz0, f
     const bool dry = ((c ? hL.y : hL.x) < kHsF && (c ? hR.y : hR.x) < kHsF) || (c ? dd1 : dd0);
     float h_ = left ? (c ? hfL.y : hfL.x) : (mid ? (c ? hfM.y : hfM.x) : (c ? hfR.y : hfR.x));
     float n_ = left ? (c ? nfL.y : nfL.x) : (mid ? (c ? nfM.y : nfM.x) : (c ? nfR.y : nfR.x));
-    float t_ = left ? (c ? tfL.y : tfL.x)
-                    : (midL ? (c ? tML.y : tML.x) : (midR ? (c ? tMR.y : tMR.x) : (c ? tfR.y : tfR.x)));
-    if (dry) h_ = n_ = t_ = 0.f;
+    if (dry) h_ = n_ = 0.f;
+    // the tangential flux is the mass flux times the upwind side's
+    // tangential velocity in every region (the reference forms the
+    // unstarred ones as u * (v * h); (u * h) * v here: one rounding apart)
+    const float vu = (left || midL) ? (c ? vL.y : vL.x) : (c ? vR.y : vR.x);
     if (c) {
-      fh.y = h_; fn.y = n_; ft.y = t_;
+      fh.y = h_; fn.y = n_; vU.y = vu;
     } else {
-      fh.x = h_; fn.x = n_; ft.x = t_;
+      fh.x = h_; fn.x = n_; vU.x = vu;
     }
   }
+  ft = mul2(fh, vU);
 }
 
 // Two interior faces between valid cells A (minus side: west, or south) and
