@@ -267,10 +267,9 @@ __device__ __forceinline__ Fc2 face2(const Cel2 &A, const Cel2 &B, const Slp2 &s
                                      const Slp2 &sB) {
   Fc2 o;
   const bool dd0 = A.h.x < kHsF && B.h.x < kHsF, dd1 = A.h.y < kHsF && B.h.y < kHsF;
-  if (dd0 && dd1) {
-    o.fh = o.fx = o.fy = o.sa = o.sb = dup(0.f);
-    return o;
-  }
+  // no early return when both faces are dry: one branch-free block lets the
+  // compiler interleave a row's x- and y-faces (the dry faces are zeroed in
+  // face_core2 and below)
   const f2 bz = sub2(B.z, A.z);
   f2 Lh, Lz, Lqx, Lqy, Rh, Rz, Rqx, Rqy;
   if constexpr (ORDER == 2) {
