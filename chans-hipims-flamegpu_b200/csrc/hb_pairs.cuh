@@ -907,32 +907,25 @@ __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, cons
           const float hh = c ? h2.y : h2.x;
           float &qx = c ? qx2.y : qx2.x;
           float &qy = c ? qy2.y : qy2.x;
-          if (hh < kHsF) {
-            qx = 0.f;
-            qy = 0.f;
-            // (sgh, ih of a dry cell: the CFL speed below skips dry cells)
-            continue;
-          }
-          if (!((c ? nman.y : nman.x) > 0.f)) continue;
+          // The limiter as selects: a dry cell stops (q = 0), a cell without
+          // Manning friction keeps q, a wet one takes the implicit value,
+          // over-corrected (2 temp - q, clipped at a sign change) where
+          // |temp| passes 5 h sqrt(gh), and q itself is kept at |q| <= 1e-10.
+          // The values a dry or friction-free cell computes here (inf or NaN
+          // at h = 0) are never selected. Same results as the branching form,
+          // without the divergent branches around the two components.
           const float l = c ? lim.y : lim.x;
-          if (fabsf(qx) > 1.0e-10f) {
-            const float temp = c ? tx.y : tx.x;
-            if (fabsf(temp) > l) {
-              const float q2 = 2.f * temp - qx;
-              qx = (q2 * temp <= 0.f) ? 0.f : q2;
-            } else {
-              qx = temp;
-            }
-          }
-          if (fabsf(qy) > 1.0e-10f) {
-            const float temp = c ? ty.y : ty.x;
-            if (fabsf(temp) > l) {
-              const float q2 = 2.f * temp - qy;
-              qy = (q2 * temp <= 0.f) ? 0.f : q2;
-            } else {
-              qy = temp;
-            }
-          }
+          auto limit = [&](float q, float temp) {
+            const float q2 = 2.f * temp - q;
+            const float over = (q2 * temp <= 0.f) ? 0.f : q2;
+            const float t = fabsf(temp) > l ? over : temp;
+            return fabsf(q) > 1.0e-10f ? t : q;
+          };
+          const bool fr = (c ? nman.y : nman.x) > 0.f, wet = !(hh < kHsF);
+          const float nqx = limit(qx, c ? tx.y : tx.x), nqy = limit(qy, c ? ty.y : ty.x);
+          // (sgh, ih of a dry cell: the CFL speed below skips dry cells)
+          qx = wet ? (fr ? nqx : qx) : 0.f;
+          qy = wet ? (fr ? nqy : qy) : 0.f;
         }
       }
       // stores: both cells valid (every all-valid tile), else per cell
