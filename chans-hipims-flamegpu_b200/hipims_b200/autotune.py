@@ -4,7 +4,14 @@ For a batch of catchments it times a few steps of each candidate (cells per
 lane -- 2 with 32 x 64 tiles, 1 with 32 x 32 or 64 x 32 tiles -- tile height and
 resident-CTA count) on scratch copies of the catchments, keeps the fastest,
 and caches the choice in a JSON file keyed by the GPU name, the dtype and the
-batch's shape (number of instances, total cells, largest side).  The cache
+batch's shape (number of instances, total cells, largest side).
+
+Each candidate is timed after a spin-up of SPINUP_STEPS untimed steps: the
+first steps from a dry start leave most faces dry, where the one-cell kernel's
+dry-face shortcuts make it the fastest, while from the first few steps of
+rain on the two-cells-per-lane build is faster by 15-30 % on the 64-catchment
+ensemble (measured on a B200: 1.14 vs 1.11 ms per step after 3 steps,
+1.15 vs 1.33 after 8, 1.16 vs 1.50 after 20).  The cache
 lives at $HIPIMS_B200_TUNE_CACHE, default ~/.cache/hipims_b200/autotune.json.
 """
 from __future__ import annotations
@@ -23,6 +30,10 @@ DEFAULT_CANDIDATES = ({"tile": (32, 64), "minb": 4}, {"tile": (32, 64), "minb": 
                       {"tile": (32, 32), "minb": 6})
 
 
+# untimed steps before a candidate is timed (see the module docstring)
+SPINUP_STEPS = 16
+
+
 def cells_per_lane(cfg: dict) -> int:
     return int(cfg["tile"][1]) // 32
 
@@ -37,7 +48,8 @@ def batch_key(catchments: Sequence[Catchment], dtype: torch.dtype, device) -> st
     name = torch.cuda.get_device_name(device)
     cells = sum(int(c.mask.size) for c in catchments)
     side = max(max(c.mask.shape) for c in catchments)
-    return f"{name}|{str(dtype).split('.')[-1]}|n={len(catchments)}|cells={cells}|side={side}"
+    return (f"{name}|{str(dtype).split('.')[-1]}|n={len(catchments)}|cells={cells}|side={side}"
+            f"|spinup={SPINUP_STEPS}")
 
 
 def _load() -> dict:
@@ -58,8 +70,9 @@ def _store(db: dict) -> None:
 
 
 def time_config(catchments: Sequence[Catchment], dtype, device, cfg: dict, steps: int = 6,
-                warmup: int = 3) -> float:
-    """Milliseconds per step of one candidate (CUDA events, after warm-up)."""
+                warmup: int = SPINUP_STEPS) -> float:
+    """Milliseconds per step of one candidate (CUDA events, after `warmup`
+    untimed steps from the catchments' initial state)."""
     fs = FusedSolver(list(catchments), dtype=dtype, device=device, tile=cfg["tile"],
                      grid_blocks=cfg.get("grid_blocks", 0), minb=cfg.get("minb", 0))
     fs.step(warmup)
