@@ -1958,14 +1958,45 @@ int launch_rows_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   return check_launch("hb_fused_step");
 }
 
-// The two-cells-per-lane step (64 x TY tiles), with the same side-stream
-// scheduling as launch_rows_impl: general tiles on the side stream, all-valid
-// tiles on the caller's stream, both at once.
-// The general build keeps the register cap of 3 CTAs per SM (its ghost-face
-// branches spill under a tighter one); MINB caps the all-valid build.
+// The two-cells-per-lane step (64 x TY tiles).  Default (MINB 4, one CTA per
+// tile): ONE launch of pairs_mixed_kernel over both tile lists on the
+// caller's stream.  Otherwise (MINB 3, or a positive grid_blocks) the
+// two builds with the same side-stream scheduling as launch_rows_impl:
+// general tiles on the side stream, all-valid tiles on the caller's stream,
+// both at once; the general build keeps the register cap of 3 CTAs per SM
+// (its ghost-face branches spill under a tighter one) and MINB caps the
+// all-valid build.
 template <int TY, int MINB, bool SOURCES, int ORDER = 2>
 int launch_pairs_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   using S = PairSmem<TY>;
+  const int n = b->n_tiles;
+  // the list lengths come from prepare (one read-back there), so that a
+  // tile's first load is its own entry
+  int n_general = 0;
+  {
+    std::lock_guard<std::mutex> lock(g_side_mu);
+    const auto it = g_general_tiles.find(b->workspace);
+    if (it == g_general_tiles.end())
+      return set_error(HB_ERR_ARG, "hb_fused_step: run hb_fused_prepare on this workspace first");
+    n_general = std::min(std::max(it->second, 0), n);
+  }
+  const int n_valid = n - n_general;
+  char *ws = reinterpret_cast<char *>(b->workspace);
+  TilePartial *parts = reinterpret_cast<TilePartial *>(ws);
+  TilePartial *gparts = reinterpret_cast<TilePartial *>(ws + ws_partials_bytes(b->n_tiles));
+  unsigned *gcount = reinterpret_cast<unsigned *>(ws + ws_gcount_offset(b));
+  const TileEntry *entries = reinterpret_cast<const TileEntry *>(ws + ws_entries_offset(b));
+  BcTable *bct = reinterpret_cast<BcTable *>(ws + ws_bct_offset(b));
+  const CUtensorMap *maps = reinterpret_cast<const CUtensorMap *>(ws + ws_maps_offset(b));
+  if (MINB == 4 && b->grid_blocks <= 0) {
+    auto *km = pairs_mixed_kernel<TY, SOURCES, ORDER>;
+    const int rc = set_smem_attr(reinterpret_cast<const void *>(km), (int)sizeof(S));
+    if (rc) return rc;
+    for (int k = 0; k < nsteps; k++)
+      km<<<std::max(n, 1), kRowsNT, sizeof(S), st>>>(b->instances, entries, n_general, n, parts,
+                                                     gparts, gcount, bct, maps);
+    return check_launch("hb_fused_step");
+  }
   auto *kg = pairs_step_kernel<TY, 3, SOURCES, 0, ORDER>;
   auto *ka = pairs_step_kernel<TY, MINB, SOURCES, 1, ORDER>;
   int rc = set_smem_attr(reinterpret_cast<const void *>(kg), (int)sizeof(S));
@@ -1977,23 +2008,9 @@ int launch_pairs_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
       !g_side[dev].stream)
     return set_error(HB_ERR_ARG, "hb_fused_step: run hb_fused_prepare on this device first");
   const SideRes &sr = g_side[dev];
-  const int n = b->n_tiles;
-  // the list lengths come from prepare (one read-back there), so that a
-  // tile's first load is its own entry
-  const auto it = g_general_tiles.find(b->workspace);
-  if (it == g_general_tiles.end())
-    return set_error(HB_ERR_ARG, "hb_fused_step: run hb_fused_prepare on this workspace first");
-  const int n_general = std::min(std::max(it->second, 0), n), n_valid = n - n_general;
   const int grid_a = std::max(b->grid_blocks > 0 ? std::min(b->grid_blocks, n_valid) : n_valid, 1);
   const int grid_g = std::max(b->grid_blocks > 0 ? std::min(b->grid_blocks, n_general) : n_general,
                               1);
-  char *ws = reinterpret_cast<char *>(b->workspace);
-  TilePartial *parts = reinterpret_cast<TilePartial *>(ws);
-  TilePartial *gparts = reinterpret_cast<TilePartial *>(ws + ws_partials_bytes(b->n_tiles));
-  unsigned *gcount = reinterpret_cast<unsigned *>(ws + ws_gcount_offset(b));
-  const TileEntry *entries = reinterpret_cast<const TileEntry *>(ws + ws_entries_offset(b));
-  BcTable *bct = reinterpret_cast<BcTable *>(ws + ws_bct_offset(b));
-  const CUtensorMap *maps = reinterpret_cast<const CUtensorMap *>(ws + ws_maps_offset(b));
   for (int k = 0; k < nsteps; k++) {
     cudaError_t e = cudaEventRecord(sr.fork, st);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(sr.stream, sr.fork, 0);

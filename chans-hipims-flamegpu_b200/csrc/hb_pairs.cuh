@@ -1073,7 +1073,7 @@ constexpr int kPersistMinBlocks = 4;
 // A general tile of the persistent step, kept out of line so that the
 // all-valid path inlined in the kernel gets the register allocation it gets in
 // its own build (the general path's ghost faces would otherwise cost it spills).
-template <int TY, bool SOURCES>
+template <int TY, bool SOURCES, int ORDER = 2>
 __device__ __noinline__ bool pair_tile_general(PairSmem<TY> &s, unsigned &phase,
                                                const TileEntry en,
                                                const hb_instance *__restrict__ insts,
@@ -1082,7 +1082,43 @@ __device__ __noinline__ bool pair_tile_general(PairSmem<TY> &s, unsigned &phase,
                                                unsigned *__restrict__ gcount,
                                                BcTable *__restrict__ bct,
                                                const CUtensorMap *__restrict__ maps) {
-  return pair_tile<TY, SOURCES, 0>(s, phase, en, insts, partials, gparts, gcount, bct, maps);
+  return pair_tile<TY, SOURCES, 0, ORDER>(s, phase, en, insts, partials, gparts, gcount, bct,
+                                          maps);
+}
+
+// The step as ONE launch of one CTA per tile over both lists (the general
+// tiles first, then the all-valid ones).  Every CTA has the all-valid build's
+// register cap (4 CTAs per SM), so the two kinds share an SM's slots evenly;
+// with the two builds as separate launches a general CTA (its own build needs
+// ~160 registers) took the room of two all-valid ones while it ran, and the
+// second launch started its tiles late.  A general tile runs the out-of-line
+// general path and returns, so the all-valid path holds no values across a
+// call and keeps the allocation of its own build.  Same results bit for bit
+// as the two launches.
+template <int TY, bool SOURCES, int ORDER>
+__global__ void __launch_bounds__(kRowsNT, 4)
+pairs_mixed_kernel(const hb_instance *__restrict__ insts, const TileEntry *__restrict__ list,
+                   const int n_general, const int n_list, TilePartial *__restrict__ partials,
+                   TilePartial *__restrict__ gparts, unsigned *__restrict__ gcount,
+                   BcTable *__restrict__ bct, const CUtensorMap *__restrict__ maps) {
+  using S = PairSmem<TY>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  S &s = *reinterpret_cast<S *>(smem_raw);
+  if (threadIdx.x == 0) {
+    mbar_init(&s.bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  unsigned phase = 0;
+  const int k = blockIdx.x;
+  if (k < n_general) {
+    pair_tile_general<TY, SOURCES, ORDER>(s, phase, list[k], insts, partials, gparts, gcount,
+                                          bct, maps);
+    return;
+  }
+  if (k < n_list)
+    pair_tile<TY, SOURCES, 1, ORDER>(s, phase, list[k], insts, partials, gparts, gcount, bct,
+                                     maps);
 }
 
 template <int TY, bool SOURCES>

@@ -189,6 +189,37 @@ def test_fused_persistent_grid_equals_one_block_per_tile(cuda, tile):
             (cb.volume, cb.outflow_volume, cb.rain_volume)
 
 
+@pytest.mark.parametrize("order,sources", [(2, False), (2, True), (1, False), (1, True)])
+def test_fused_one_launch_equals_two_builds(cuda, order, sources):
+    """The default 64-wide step is ONE launch over both tile lists
+    (pairs_mixed_kernel, general tiles through the out-of-line general path);
+    a positive grid_blocks launches the general-tile and all-valid-tile builds
+    on two streams instead.  Same tile code, so fields, clocks and volumes are
+    equal bit for bit, in both schemes, with and without the per-cell source
+    terms (infiltration)."""
+    from hipims_b200 import scenarios as S
+    from hipims_b200.fused import FusedSolver
+
+    ds = [S.urban_catchment(n, seed=k + 30, rain_mm_h=100.0) for k, n in enumerate((300, 90))]
+    over = {"infiltration": dict(INFIL)} if sources else {}
+    cs = [catchment(d, **over) for d in ds]
+    a = FusedSolver(cs, dtype=torch.float32, device=cuda, tile=(32, 64), order=order)
+    b = FusedSolver(cs, dtype=torch.float32, device=cuda, tile=(32, 64), order=order,
+                    grid_blocks=1 << 20)
+    a.step(40)
+    b.step(40)
+    a.check()
+    b.check()
+    for k in range(len(cs)):
+        x, y = a.compacted(k), b.compacted(k)
+        for f in x:
+            np.testing.assert_array_equal(x[f], y[f])
+        ca, cb = a.controls()[k], b.controls()[k]
+        assert (ca.t, ca.dt, ca.step) == (cb.t, cb.dt, cb.step)
+        assert (ca.volume, ca.outflow_volume, ca.rain_volume) == \
+            (cb.volume, cb.outflow_volume, cb.rain_volume)
+
+
 def test_fused_graph_replay_equals_eager(cuda):
     from hipims_b200 import scenarios as S
     from hipims_b200.fused import FusedSolver
