@@ -1797,60 +1797,64 @@ classify_tiles_kernel(const hb_instance *__restrict__ insts, const int32_t *__re
 }
 
 // Stable partition of the tiles by flag, one block: order = general tiles
-// (flags 0 and 2) in index order, then all-valid tiles (flag 1) in index
-// order; counts = {general, all-valid}.  A flag-2 tile (no valid cell) is
-// listed as ~tile.
+// with a valid cell (flag 0) in index order, then all-valid tiles (flag 1) in
+// index order, then the tiles without a valid cell (flag 2, 64-wide tiles
+// only) in index order, listed as ~tile; counts = {general (flags 0 and 2),
+// all-valid, no valid cell}.  The tiles without a valid cell come last so
+// that the one-launch step dispatches them at its end, where they take slots
+// the last wave of tiles leaves idle.
 constexpr int kOrderNT = 1024;
 __global__ void __launch_bounds__(kOrderNT)
 order_tiles_kernel(const uint8_t *__restrict__ flags, int n, int32_t *__restrict__ order,
                    int32_t *__restrict__ counts) {
-  __shared__ int s_g[kOrderNT / 32], s_a[kOrderNT / 32];
-  __shared__ int s_total, s_base[2];
+  __shared__ int s_c[3][kOrderNT / 32];
+  __shared__ int s_total[3], s_base[3];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  if (tid == 0) s_total = 0;
+  if (tid < 3) s_total[tid] = 0;
   __syncthreads();
-  int cnt = 0;
-  for (int i = tid; i < n; i += kOrderNT) cnt += flags[i] != 1;
-  atomicAdd(&s_total, cnt);
+  int c0 = 0, c1 = 0;
+  for (int i = tid; i < n; i += kOrderNT) {
+    c0 += flags[i] == 0;
+    c1 += flags[i] == 1;
+  }
+  atomicAdd(&s_total[0], c0);
+  atomicAdd(&s_total[1], c1);
   __syncthreads();
   if (tid == 0) {
+    s_total[2] = n - s_total[0] - s_total[1];
     s_base[0] = 0;
-    s_base[1] = s_total;
+    s_base[1] = s_total[0];
+    s_base[2] = s_total[0] + s_total[1];
   }
   __syncthreads();
   const unsigned below = (1u << lane) - 1u;
   for (int c = 0; c < n; c += kOrderNT) {
     const int i = c + tid;
-    const int f = i < n ? flags[i] : 3;  // past the end: in neither list
-    const unsigned bg = __ballot_sync(0xffffffffu, f == 0 || f == 2);
-    const unsigned ba = __ballot_sync(0xffffffffu, f == 1);
-    if (lane == 0) {
-      s_g[w] = __popc(bg);
-      s_a[w] = __popc(ba);
+    const int f = i < n ? flags[i] : 3;  // past the end: in no list
+    unsigned bal[3];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      bal[q] = __ballot_sync(0xffffffffu, f == q);
+      if (lane == 0) s_c[q][w] = __popc(bal[q]);
     }
     __syncthreads();
-    int og = 0, oa = 0;  // warps before this one
-    for (int q = 0; q < w; q++) {
-      og += s_g[q];
-      oa += s_a[q];
+    if (f < 3) {
+      int o = 0;  // this flag's tiles in the warps before this one
+      for (int q = 0; q < w; q++) o += s_c[f][q];
+      order[s_base[f] + o + __popc(bal[f] & below)] = f == 2 ? ~i : i;
     }
-    if (f == 0 || f == 2) order[s_base[0] + og + __popc(bg & below)] = f == 2 ? ~i : i;
-    if (f == 1) order[s_base[1] + oa + __popc(ba & below)] = i;
     __syncthreads();
-    if (tid == 0) {
-      int tg = 0, ta = 0;
-      for (int q = 0; q < kOrderNT / 32; q++) {
-        tg += s_g[q];
-        ta += s_a[q];
-      }
-      s_base[0] += tg;
-      s_base[1] += ta;
+    if (tid < 3) {
+      int t = 0;
+      for (int q = 0; q < kOrderNT / 32; q++) t += s_c[tid][q];
+      s_base[tid] += t;
     }
     __syncthreads();
   }
   if (tid == 0) {
-    counts[0] = s_total;
-    counts[1] = n - s_total;
+    counts[0] = s_total[0] + s_total[2];
+    counts[1] = s_total[1];
+    counts[2] = s_total[2];
   }
 }
 
@@ -1881,9 +1885,13 @@ struct SideRes {
 };
 std::mutex g_side_mu;
 SideRes g_side[kMaxSideDevices];
-// counts of general tiles per prepared workspace (read back at prepare), so
-// that the general-tile kernel gets one CTA per tile; guarded by g_side_mu
-std::unordered_map<const void *, int> g_general_tiles;
+// counts of general tiles (with or without a valid cell) and of the tiles
+// without a valid cell, per prepared workspace (read back at prepare), so
+// that the step launches one CTA per tile; guarded by g_side_mu
+struct TileCounts {
+  int general = 0, empty = 0;
+};
+std::unordered_map<const void *, TileCounts> g_general_tiles;
 
 int side_setup() {
   int dev = 0;
@@ -1932,7 +1940,7 @@ int launch_rows_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   const int n = b->n_tiles;
   int n_general = n;  // unknown workspace: CTAs beyond the general count exit at once
   const auto it = g_general_tiles.find(b->workspace);
-  if (it != g_general_tiles.end()) n_general = std::max(it->second, 1);
+  if (it != g_general_tiles.end()) n_general = std::max(it->second.general, 1);
   const int grid_a = b->grid_blocks > 0 ? std::min(b->grid_blocks, n) : n;
   const int grid_g = b->grid_blocks > 0 ? std::min(b->grid_blocks, n) : std::min(n_general, n);
   char *ws = reinterpret_cast<char *>(b->workspace);
@@ -1972,15 +1980,18 @@ int launch_pairs_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
   const int n = b->n_tiles;
   // the list lengths come from prepare (one read-back there), so that a
   // tile's first load is its own entry
-  int n_general = 0;
+  // entries: general tiles with a valid cell [0, n_live), all-valid tiles
+  // [n_live, n_live + n_valid), tiles without a valid cell [.., n)
+  int n_general = 0, n_empty = 0;
   {
     std::lock_guard<std::mutex> lock(g_side_mu);
     const auto it = g_general_tiles.find(b->workspace);
     if (it == g_general_tiles.end())
       return set_error(HB_ERR_ARG, "hb_fused_step: run hb_fused_prepare on this workspace first");
-    n_general = std::min(std::max(it->second, 0), n);
+    n_general = std::min(std::max(it->second.general, 0), n);
+    n_empty = std::min(std::max(it->second.empty, 0), n_general);
   }
-  const int n_valid = n - n_general;
+  const int n_valid = n - n_general, n_live = n_general - n_empty;
   char *ws = reinterpret_cast<char *>(b->workspace);
   TilePartial *parts = reinterpret_cast<TilePartial *>(ws);
   TilePartial *gparts = reinterpret_cast<TilePartial *>(ws + ws_partials_bytes(b->n_tiles));
@@ -1993,8 +2004,9 @@ int launch_pairs_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
     const int rc = set_smem_attr(reinterpret_cast<const void *>(km), (int)sizeof(S));
     if (rc) return rc;
     for (int k = 0; k < nsteps; k++)
-      km<<<std::max(n, 1), kRowsNT, sizeof(S), st>>>(b->instances, entries, n_general, n, parts,
-                                                     gparts, gcount, bct, maps);
+      km<<<std::max(n, 1), kRowsNT, sizeof(S), st>>>(b->instances, entries, n_live,
+                                                     n_live + n_valid, n, parts, gparts, gcount,
+                                                     bct, maps);
     return check_launch("hb_fused_step");
   }
   auto *kg = pairs_step_kernel<TY, 3, SOURCES, 0, ORDER>;
@@ -2015,10 +2027,11 @@ int launch_pairs_impl(const hb_fused_batch *b, int nsteps, cudaStream_t st) {
     cudaError_t e = cudaEventRecord(sr.fork, st);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(sr.stream, sr.fork, 0);
     if (e != cudaSuccess) return set_error(HB_ERR_CUDA, "hb_fused_step fork: %s", cudaGetErrorString(e));
-    kg<<<grid_g, kRowsNT, sizeof(S), sr.stream>>>(b->instances, entries, n_general, parts, gparts,
-                                                  gcount, bct, maps);
-    ka<<<grid_a, kRowsNT, sizeof(S), st>>>(b->instances, entries + n_general, n_valid, parts,
-                                           gparts, gcount, bct, maps);
+    // the general build skips the all-valid entries in the middle of the list
+    kg<<<grid_g, kRowsNT, sizeof(S), sr.stream>>>(b->instances, entries, n_general, n_live,
+                                                  n_valid, parts, gparts, gcount, bct, maps);
+    ka<<<grid_a, kRowsNT, sizeof(S), st>>>(b->instances, entries + n_live, n_valid, n_valid, 0,
+                                           parts, gparts, gcount, bct, maps);
     e = cudaEventRecord(sr.join, sr.stream);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(st, sr.join, 0);
     if (e != cudaSuccess) return set_error(HB_ERR_CUDA, "hb_fused_step join: %s", cudaGetErrorString(e));
@@ -2218,14 +2231,14 @@ int prepare_impl(const hb_fused_batch *b, cudaStream_t st, CUtensorMap *host_map
       tile_entries_kernel<<<(b->n_tiles + 255) / 256, 256, 0, st>>>(
           reinterpret_cast<const int32_t *>(ws + ws_order_offset(b)), b->n_tiles,
           b->tile_instance, b->instances, reinterpret_cast<TileEntry *>(ws + ws_entries_offset(b)));
-    int32_t counts[2] = {0, 0};
+    int32_t counts[3] = {0, 0, 0};
     cudaError_t e = cudaMemcpyAsync(counts, ws + ws_counts_offset(b), sizeof(counts),
                                     cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess)
       return set_error(HB_ERR_CUDA, "hb_fused_prepare: tile classes: %s", cudaGetErrorString(e));
     std::lock_guard<std::mutex> lock(g_side_mu);
-    g_general_tiles[b->workspace] = counts[0];
+    g_general_tiles[b->workspace] = TileCounts{counts[0], counts[2]};
   }
   // blocks per instance for the volume sum: about 16 cells per thread of the
   // largest instance (the host copy of the records gives the sizes)

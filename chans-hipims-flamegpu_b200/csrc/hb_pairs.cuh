@@ -1031,11 +1031,14 @@ __device__ __forceinline__ bool pair_tile(PairSmem<TY> &s, unsigned &phase, cons
 }
 
 // The step kernel: one launch per step and build, one CTA per tile by
-// default (a positive grid loops over the build's tiles).
+// default (a positive grid loops over the build's tiles).  Tile k of the
+// launch is list[k] before gap_at and list[k + gap_len] from there on (the
+// general build skips the all-valid entries between its two parts).
 template <int TY, int MINB, bool SOURCES, int PATH, int ORDER = 2>
 __global__ void __launch_bounds__(kRowsNT, MINB)
 pairs_step_kernel(const hb_instance *__restrict__ insts, const TileEntry *__restrict__ list,
-                  const int n_list, TilePartial *__restrict__ partials,
+                  const int n_list, const int gap_at, const int gap_len,
+                  TilePartial *__restrict__ partials,
                   TilePartial *__restrict__ gparts,
                   unsigned *__restrict__ gcount, BcTable *__restrict__ bct,
                   const CUtensorMap *__restrict__ maps) {
@@ -1049,15 +1052,16 @@ pairs_step_kernel(const hb_instance *__restrict__ insts, const TileEntry *__rest
   __syncthreads();
   unsigned phase = 0;
   for (int k = blockIdx.x; k < n_list; k += gridDim.x)
-    if (!pair_tile<TY, SOURCES, PATH, ORDER>(s, phase, list[k], insts, partials, gparts, gcount,
-                                             bct, maps))
+    if (!pair_tile<TY, SOURCES, PATH, ORDER>(s, phase, list[k < gap_at ? k : k + gap_len], insts,
+                                             partials, gparts, gcount, bct, maps))
       return;
 }
 
 // ===========================================================================
 // The persistent step: every instance of a batch advanced by nsteps steps in
 // ONE cooperative launch of resident CTAs.  Per step, CTAs take tiles from a
-// global counter in the prepared order (general tiles first), each tile runs
+// global counter in the prepared order (general tiles with a valid cell
+// first, the tiles without one last), each tile runs
 // exactly as in the per-step kernel (its instance's last tile finalizes the
 // clock), and a grid barrier ends the step.  The barrier wait is bounded by
 // `budget` clock cycles: a CTA that gives up sets the give-up flag and bit 8
@@ -1086,8 +1090,10 @@ __device__ __noinline__ bool pair_tile_general(PairSmem<TY> &s, unsigned &phase,
                                           maps);
 }
 
-// The step as ONE launch of one CTA per tile over both lists (the general
-// tiles first, then the all-valid ones).  Every CTA has the all-valid build's
+// The step as ONE launch of one CTA per tile over the whole list: general
+// tiles with a valid cell [0, n_live), all-valid tiles [n_live, n_valid_end),
+// then the general tiles without a valid cell, which only add a zero partial
+// and so take the slots the last wave leaves idle.  Every CTA has the all-valid build's
 // register cap (4 CTAs per SM), so the two kinds share an SM's slots evenly;
 // with the two builds as separate launches a general CTA (its own build needs
 // ~160 registers) took the room of two all-valid ones while it ran, and the
@@ -1098,7 +1104,8 @@ __device__ __noinline__ bool pair_tile_general(PairSmem<TY> &s, unsigned &phase,
 template <int TY, bool SOURCES, int ORDER>
 __global__ void __launch_bounds__(kRowsNT, 4)
 pairs_mixed_kernel(const hb_instance *__restrict__ insts, const TileEntry *__restrict__ list,
-                   const int n_general, const int n_list, TilePartial *__restrict__ partials,
+                   const int n_live, const int n_valid_end, const int n_list,
+                   TilePartial *__restrict__ partials,
                    TilePartial *__restrict__ gparts, unsigned *__restrict__ gcount,
                    BcTable *__restrict__ bct, const CUtensorMap *__restrict__ maps) {
   using S = PairSmem<TY>;
@@ -1111,12 +1118,12 @@ pairs_mixed_kernel(const hb_instance *__restrict__ insts, const TileEntry *__res
   __syncthreads();
   unsigned phase = 0;
   const int k = blockIdx.x;
-  if (k < n_general) {
+  if (k < n_live || (k >= n_valid_end && k < n_list)) {
     pair_tile_general<TY, SOURCES, ORDER>(s, phase, list[k], insts, partials, gparts, gcount,
                                           bct, maps);
     return;
   }
-  if (k < n_list)
+  if (k < n_valid_end)
     pair_tile<TY, SOURCES, 1, ORDER>(s, phase, list[k], insts, partials, gparts, gcount, bct,
                                      maps);
 }
