@@ -536,7 +536,7 @@ def ensemble_rate(dev, steps: int, count: int = 64, seed: int = 0, plain_sample:
     """Config 3: `count` catchments (sides 256-1536, own hyetographs) advanced
     together.  `value`: one persistent cooperative launch of `steps` steps for
     all of them (hb_fused_run), replayed from a CUDA graph.  Beside it: the
-    same batch as one graph of `steps` per-step launch pairs, the autotuned
+    same batch as one graph of `steps` per-step launches, the autotuned
     launch shape, 64 sequential single-instance fused runs, and the plain FP64
     path (the reference's solver class on its own kernels) on a sample of the
     catchments run one after another."""
@@ -569,7 +569,7 @@ def ensemble_rate(dev, steps: int, count: int = 64, seed: int = 0, plain_sample:
     fp.check()
     del fp
     torch.cuda.empty_cache()
-    # per-step launch pairs, autotuned shape, replayed from a graph
+    # per-step launches, autotuned shape, replayed from a graph
     fs = FusedSolver(cs, dtype=torch.float32, device=dev, tile=cfg["tile"],
                      minb=cfg.get("minb", 0))
     fs.step(SPINUP)
@@ -614,8 +614,9 @@ def ensemble_rate(dev, steps: int, count: int = 64, seed: int = 0, plain_sample:
            "per_step_launches": {"value": cells * steps / (ms_s * 1e-3) / 1e9, "unit": METRIC,
                                  "tile": list(cfg["tile"]), "minb": cfg.get("minb", 0),
                                  "cells_per_lane": autotune.cells_per_lane(cfg),
-                                 "launch": f"one CUDA-graph replay of {steps} per-step launch "
-                                           f"pairs (autotuned shape)"},
+                                 "launch": f"one CUDA-graph replay of {steps} per-step launches "
+                                           f"(autotuned shape: one launch per step for 64-wide "
+                                           f"tiles at 4 CTAs per SM, a pair otherwise)"},
            "sequential_single_runs": {"value": cells * steps / (ms_seq * 1e-3) / 1e9,
                                       "unit": METRIC,
                                       "path": f"{count} single-instance fused FP32 runs, one "
