@@ -521,8 +521,8 @@ def first_order_rates(d: dict, dev, args, flush: torch.Tensor, stream, steps: in
     ms = sum(a.elapsed_time(b) for a, b in ev) / steps
     value = n / (ms * 1e-3) / 1e9
     out = {"value": value, "unit": METRIC, "steps": steps, "ms_per_step": ms, "dtype": "f32",
-           "path": "FusedSolver(order=1), 64 x 32 tiles, two cells per lane: the two builds "
-                   "of the 1st-order step kernel, "
+           "path": "FusedSolver(order=1), 64 x 32 tiles, two cells per lane: one launch per "
+                   "step of the 1st-order step kernel over the general and all-valid tiles, "
                    "CUDA events per step, L2 flushed between steps"}
     del fs
     pl = plain_fp64_rate(d, dev, reference_kernels=True, order=1)
