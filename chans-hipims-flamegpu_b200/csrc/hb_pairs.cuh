@@ -20,7 +20,12 @@
 //    cell 2j+1 comes from lane j+1 by one shuffle per value (lane 31: a
 //    tile-edge pre-pass), so shuffles and loop overhead are per cell pair;
 //  * the cell update (activity, rain, implicit friction, h_max, CFL speed,
-//    FP64 volume) runs on the pair, packed where the arithmetic allows.
+//    FP64 volume) runs on the pair, packed where the arithmetic allows;
+//  * a step is one launch of pairs_mixed_kernel, one CTA per tile over the
+//    prepared list (general tiles with a valid cell, all-valid tiles, tiles
+//    without a valid cell), every CTA at the all-valid build's register cap;
+//    pairs_step_kernel keeps the general and all-valid builds as two launches
+//    for a 3-CTA register cap or a looping grid.
 // Every packed operation is pinned by inline PTX (no contraction freedom), and
 // all faces -- interior, tile-edge and ghost -- go through the same packed
 // function, so a face evaluated by two tiles, or by the general and the
