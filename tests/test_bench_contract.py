@@ -32,3 +32,23 @@ def test_reference_arm_other_ranks_exit_quietly():
                          capture_output=True, text=True, timeout=300, cwd=ROOT, env=env)
     assert out.returncode == 0
     assert not [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+
+
+def test_launch_count_claim_follows_the_launch_form():
+    """The GPU arm's `gpu_launches` claim: one launch per step for 64-wide tiles
+    at the default register cap (pairs_mixed_kernel), the two builds for a
+    3-CTA cap and for 32-wide tiles."""
+    import argparse
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    def args(tile, minb):
+        return argparse.Namespace(tile=list(tile), minb=minb)
+
+    assert bench.one_launch_step(args((32, 64), 0)) and bench.one_launch_step(args((32, 64), 4))
+    assert not bench.one_launch_step(args((32, 64), 3))
+    assert not bench.one_launch_step(args((32, 32), 0))
+    assert bench.step_kernel_name(args((32, 64), 0)).startswith("pairs_mixed_kernel")
+    assert bench.step_kernel_name(args((32, 64), 3)).startswith("pairs_step_kernel")
+    assert bench.step_kernel_name(args((32, 32), 5)).startswith("rows_step_kernel")
